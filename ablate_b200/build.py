@@ -1,0 +1,93 @@
+"""Build the in-tree shared libraries.
+
+* ``ablate_b200/lib/libablate_fv.so`` -- the product: sm_100a CUDA kernels behind the C ABI of
+  ``include/ablate_fv.h`` (nvcc, ``-gencode arch=compute_100a,code=sm_100a``).
+* ``oracle/liborc.so`` -- the CPU oracle used by the tests and the CPU baseline (g++ -O3, OpenMP).
+
+Both are plain ``nvcc``/``g++`` invocations; nothing is JIT-compiled at import time, so the built
+files travel with the source tree to the machine that runs them.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "ablate_b200"
+CSRC = PKG / "csrc"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libablate_fv.so"
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_LIB = ORACLE_DIR / "liborc.so"
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+    "--expt-relaxed-constexpr",
+    "-Xptxas", "-warn-spills",
+]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: Path, sources: list[Path]) -> bool:
+    if not target.exists():
+        return False
+    t = target.stat().st_mtime
+    return all(s.stat().st_mtime <= t for s in sources)
+
+
+def build_product(force: bool = False, verbose: bool = False) -> Path:
+    sources = sorted(CSRC.glob("*.cu"))
+    deps = sources + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [ROOT / "include" / "ablate_fv.h"]
+    if not force and _newer(LIB, deps):
+        return LIB
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    objdir = LIBDIR / "obj"
+    objdir.mkdir(exist_ok=True)
+    objs = []
+    for src in sources:
+        obj = objdir / (src.stem + ".o")
+        cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(LIB), "-lcudart"]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+def build_oracle(force: bool = False, verbose: bool = False) -> Path:
+    sources = [ORACLE_DIR / "oracle.cpp"]
+    deps = sources + [ORACLE_DIR / "oracle.h", ROOT / "include" / "ablate_fv.h"]
+    if not force and _newer(ORACLE_LIB, deps):
+        return ORACLE_LIB
+    cmd = ["g++", "-O3", "-march=native", "-fopenmp", "-std=c++17", "-shared", "-fPIC",
+           *map(str, sources), "-o", str(ORACLE_LIB)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return ORACLE_LIB
+
+
+def main(argv: list[str]) -> int:
+    force = "--force" in argv
+    verbose = "-v" in argv
+    build_oracle(force, verbose)
+    build_product(force, verbose)
+    print(f"built {LIB} and {ORACLE_LIB}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

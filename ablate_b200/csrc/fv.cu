@@ -1,0 +1,614 @@
+// fv.cu -- C ABI of the B200 finite-volume RHS backend (declared in include/ablate_fv.h): handle
+// lifecycle, device residency of mesh/geometry/weights, kernel dispatch and the device batch entry
+// points used by the known-answer tests.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fv_kernels.cuh"
+#include "fv_setup.hpp"
+
+namespace abl {
+
+thread_local std::string g_last_error;
+
+struct AblError : std::runtime_error {
+    int code;
+    AblError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define ABL_CUDA(call)                                                                                           \
+    do {                                                                                                         \
+        cudaError_t e_ = (call);                                                                                 \
+        if (e_ != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw AblError(e == cudaErrorMemoryAllocation ? ABL_ERR_OUT_OF_MEMORY : ABL_ERR_CUDA,
+                           std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+    }
+    void upload(const T* h, size_t count) {
+        alloc(count);
+        if (count) ABL_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    void zero() {
+        if (n) ABL_CUDA(cudaMemset(p, 0, n * sizeof(T)));
+    }
+};
+
+}  // namespace abl
+
+using namespace abl;
+
+struct abl_fv {
+    int device = 0;
+    int dim = 0, ns = 0, nc = 0, naux = 0;
+    int n_cells = 0, n_faces = 0, n_flux_faces = 0;
+    Phys phys{};
+    DevMesh mesh{};
+    // resident mesh + geometry
+    DevBuf<int2> face_cells;
+    DevBuf<uint8_t> kind, cone_side, face_boundary;
+    DevBuf<int> cone_ptr, cone_face, cone_nbr, flux_faces;
+    DevBuf<double> normal, fdx, vol, cgrad, fgrad;
+    DevBuf<double> nasa7, mw, inv_mw, href;
+    // work buffers
+    DevBuf<double> aux, fflux;
+    DevBuf<double> grad64, agrad64;
+    DevBuf<float> grad32, agrad32;
+    DevBuf<int> status;
+    // host-pointer path
+    DevBuf<double> hU, hF;
+    bool need_aux = false, need_state_grad = false, need_aux_grad = false;
+};
+
+namespace {
+
+int fail(const AblError& e) {
+    g_last_error = e.what();
+    return e.code;
+}
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F&& fn) {
+    try {
+        fn();
+        return ABL_OK;
+    } catch (const AblError& e) {
+        return fail(e);
+    } catch (const std::invalid_argument& e) {
+        return fail(ABL_ERR_INVALID_ARGUMENT, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(ABL_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(ABL_ERR_INVALID_ARGUMENT, e.what());
+    }
+}
+
+inline unsigned blocks_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+void check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+// host NASA-7 molar enthalpy, same polynomial as the device
+double host_h_molar(const double* c, double T) {
+    const double* a = (T < c[0]) ? c + 1 : c + 8;
+    return kRuniv * T * (a[0] + T * (a[1] * 0.5 + T * (a[2] * (1.0 / 3.0) + T * (a[3] * 0.25 + T * a[4] * 0.2))) + a[5] / T);
+}
+
+void validate_physics(const abl_physics_desc* p) {
+    if (!p) throw std::invalid_argument("physics descriptor is NULL");
+    if (p->eos != ABL_EOS_PERFECT_GAS && p->eos != ABL_EOS_NASA7) throw std::invalid_argument("unknown eos");
+    if (p->n_species < 0 || p->n_species > 64) throw std::invalid_argument("n_species out of range");
+    if (p->eos == ABL_EOS_NASA7 && (p->n_species < 1 || !p->nasa7 || !p->mw)) throw std::invalid_argument("NASA-7 EOS needs n_species >= 1, nasa7 and mw");
+    if (p->eos == ABL_EOS_PERFECT_GAS && !(p->gamma > 1.0 && p->r_gas > 0.0)) throw std::invalid_argument("perfect gas needs gamma > 1 and r_gas > 0");
+    if (p->flux < ABL_FLUX_OFF || p->flux > ABL_FLUX_RIEMANN) throw std::invalid_argument("unknown flux calculator");
+    if (p->flux == ABL_FLUX_RIEMANN && p->eos != ABL_EOS_PERFECT_GAS)
+        throw std::invalid_argument("Riemann flux only accepts EOS of type eos::PerfectGas");  // riemann.cpp:37-43
+    if (p->reconstruction != ABL_RECON_UPWIND && p->reconstruction != ABL_RECON_LEASTSQUARES) throw std::invalid_argument("unknown reconstruction");
+    if (p->limiter < ABL_LIMITER_NONE || p->limiter > ABL_LIMITER_SIN) throw std::invalid_argument("unknown limiter");
+    if (p->transport < ABL_TRANSPORT_NONE || p->transport > ABL_TRANSPORT_CONSTANT_LEWIS) throw std::invalid_argument("unknown transport model");
+}
+
+Phys make_phys(const abl_physics_desc* p) {
+    Phys P{};
+    P.eos = p->eos;
+    P.ns = p->n_species;
+    P.flux = p->flux;
+    P.recon = p->reconstruction;
+    P.limiter = p->limiter;
+    P.transport = p->transport;
+    P.advection = p->advection;
+    P.diffusion = p->diffusion;
+    P.sp_adv = p->species_advection;
+    P.sp_dif = p->species_diffusion;
+    P.gamma = p->gamma;
+    P.r_gas = p->r_gas;
+    P.minf = p->ausmpup_minf;
+    P.alpha = p->pgs_alpha > 0 ? p->pgs_alpha : 1.0;
+    P.max_lim_grad = p->max_lim_grad > 0 ? p->max_lim_grad : 1e10;
+    P.k = p->k;
+    P.mu = p->mu;
+    P.diff = p->diff;
+    return P;
+}
+
+// upload NASA-7 tables and derived per-species constants; fills P's device pointers
+void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, DevBuf<double>& mw, DevBuf<double>& inv_mw, DevBuf<double>& href) {
+    if (p->eos != ABL_EOS_NASA7) return;
+    const int ns = p->n_species;
+    std::vector<double> imw(ns), hr(ns);
+    for (int k = 0; k < ns; k++) {
+        if (!(p->mw[k] > 0)) throw std::invalid_argument("molar mass must be positive");
+        imw[k] = 1.0 / p->mw[k];
+        hr[k] = host_h_molar(p->nasa7 + 15 * k, kTref) / p->mw[k];  // TChemBase reference enthalpy (tChemBase.cpp:43-69)
+    }
+    nasa7.upload(p->nasa7, (size_t)ns * 15);
+    mw.upload(p->mw, ns);
+    inv_mw.upload(imw.data(), ns);
+    href.upload(hr.data(), ns);
+    P.nasa7 = nasa7.p;
+    P.mw = mw.p;
+    P.inv_mw = inv_mw.p;
+    P.href = href.p;
+}
+
+// ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
+template <int DIM, int NS>
+void run_rhs(abl_fv* fv, const double* U, double* F, int precision, cudaStream_t s) {
+    const DevMesh& M = fv->mesh;
+    const Phys& P = fv->phys;
+    if (fv->need_aux) {
+        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, P, U, fv->aux.p, fv->status.p);
+        check_launch();
+    }
+    if (precision == ABL_PRECISION_MIXED) {
+        if (fv->need_state_grad || fv->need_aux_grad) {
+            k_gradient<DIM, NS, float><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad32.p, fv->agrad32.p,
+                                                                                   fv->need_state_grad, fv->need_aux_grad);
+            check_launch();
+        }
+        if (M.n_flux_faces > 0) {
+            k_face_flux<DIM, NS, float><<<blocks_for(M.n_flux_faces, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad32.p, fv->agrad32.p,
+                                                                                          fv->fflux.p, fv->status.p);
+            check_launch();
+        }
+    } else {
+        if (fv->need_state_grad || fv->need_aux_grad) {
+            k_gradient<DIM, NS, double><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p,
+                                                                                    fv->need_state_grad, fv->need_aux_grad);
+            check_launch();
+        }
+        if (M.n_flux_faces > 0) {
+            k_face_flux<DIM, NS, double><<<blocks_for(M.n_flux_faces, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p,
+                                                                                           fv->fflux.p, fv->status.p);
+            check_launch();
+        }
+    }
+    k_gather<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, fv->fflux.p, F, fv->status.p);
+    check_launch();
+}
+
+void dispatch_rhs(abl_fv* fv, const double* U, double* F, int precision, cudaStream_t s) {
+    const int key = fv->dim * 100 + fv->ns;
+    switch (key) {
+        case 100: return run_rhs<1, 0>(fv, U, F, precision, s);
+        case 200: return run_rhs<2, 0>(fv, U, F, precision, s);
+        case 202: return run_rhs<2, 2>(fv, U, F, precision, s);
+        case 300: return run_rhs<3, 0>(fv, U, F, precision, s);
+        case 302: return run_rhs<3, 2>(fv, U, F, precision, s);
+        case 305: return run_rhs<3, 5>(fv, U, F, precision, s);
+        case 309: return run_rhs<3, 9>(fv, U, F, precision, s);
+    }
+    throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for dim " + std::to_string(fv->dim) + " with " + std::to_string(fv->ns) +
+                                            " species (compiled: dim 1/2/3 without species, dim 2 with 2, dim 3 with 2, 5 or 9)");
+}
+
+bool rhs_supported(int dim, int ns) {
+    const int key = dim * 100 + ns;
+    return key == 100 || key == 200 || key == 202 || key == 300 || key == 302 || key == 305 || key == 309;
+}
+
+// ---- batch kernels ------------------------------------------------------------------------------
+__global__ void k_flux_batch(Phys P, int64_t n, const double* uL, const double* aL, const double* rhoL, const double* pL, const double* uR,
+                             const double* aR, const double* rhoR, const double* pR, double* mf, double* p12, int32_t* dir, int* status) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool ok = true;
+    double m, p;
+    dir[i] = flux_calc<double>(P, uL[i], aL[i], rhoL[i], pL[i], uR[i], aR[i], rhoR[i], pR[i], &m, p12 ? &p : nullptr, &ok);
+    mf[i] = m;
+    if (p12) p12[i] = p;
+    if (!ok) atomicOr(status, kStatusRiemann);
+}
+
+template <int DIM>
+__device__ void eos_property(const Phys& P, int ns, int prop, const double* U, bool hasT, double Tin, double* out, bool* ok) {
+    const double rho = U[0];
+    const bool pg = P.eos == ABL_EOS_PERFECT_GAS;
+    const double g = P.gamma, Rg = P.r_gas;
+    if (!hasT) {
+        if (pg) {
+            const double e = internal_energy<DIM>(U);
+            if (prop == ABL_PROP_PRESSURE) {
+                *out = (g - 1.0) * rho * e;
+                return;
+            }
+            if (prop == ABL_PROP_INTERNAL_SENSIBLE_ENERGY) {
+                *out = e;
+                return;
+            }
+            if (prop == ABL_PROP_SPEED_OF_SOUND) {
+                const double pr = (g - 1.0) * rho * e;
+                *out = sqrt(g * (pr) / rho);
+                return;
+            }
+        } else if (prop == ABL_PROP_INTERNAL_SENSIBLE_ENERGY) {
+            *out = internal_energy<DIM>(U);
+            return;
+        }
+        Tin = temperature<DIM, 64>(P, ns, U, 300.0, ok);
+        if (prop == ABL_PROP_TEMPERATURE) {
+            *out = Tin;
+            return;
+        }
+    }
+    const double T = Tin;
+    if (pg) {
+        switch (prop) {
+            case ABL_PROP_PRESSURE: *out = Rg * rho * T; return;
+            case ABL_PROP_TEMPERATURE: *out = temperature<DIM, 0>(P, 0, U, T, ok); return;
+            case ABL_PROP_INTERNAL_SENSIBLE_ENERGY: *out = T * (Rg / (g - 1.0)); return;
+            case ABL_PROP_SENSIBLE_ENTHALPY: *out = T * (g * Rg / (g - 1.0)); return;
+            case ABL_PROP_CV: *out = Rg / (g - 1.0); return;
+            case ABL_PROP_CP: *out = g * Rg / (g - 1.0); return;
+            case ABL_PROP_SPEED_OF_SOUND: {
+                const double pr = Rg * rho * T;
+                *out = sqrt(g * (pr) / rho);
+                return;
+            }
+            case ABL_PROP_SPECIES_SENSIBLE_ENTHALPY:
+                for (int s = 0; s < ns; s++) out[s] = 0.0;
+                return;
+            case ABL_PROP_DENSITY: *out = rho; return;
+        }
+        return;
+    }
+    double ys[64];
+    fill_y(ns, rho, U + 2 + DIM, ys);
+    switch (prop) {
+        case ABL_PROP_PRESSURE: *out = rho * kRuniv * T / mixture_mw(P, ns, ys); return;
+        case ABL_PROP_TEMPERATURE: *out = temperature<DIM, 64>(P, ns, U, T, ok); return;
+        case ABL_PROP_INTERNAL_SENSIBLE_ENERGY: *out = e_sens(P, ns, ys, T); return;
+        case ABL_PROP_SENSIBLE_ENTHALPY: {
+            double h = 0;
+            for (int k = 0; k < ns; k++) h += (nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k]) * ys[k];
+            *out = h;
+            return;
+        }
+        case ABL_PROP_CV: *out = mixture_cp(P, ns, ys, T) - kRuniv / mixture_mw(P, ns, ys); return;
+        case ABL_PROP_CP: *out = mixture_cp(P, ns, ys, T); return;
+        case ABL_PROP_SPEED_OF_SOUND: {
+            const double cp = mixture_cp(P, ns, ys, T);
+            const double R = kRuniv / mixture_mw(P, ns, ys);
+            const double cv = cp - R;
+            *out = sqrt(cp / cv * R * T);
+            return;
+        }
+        case ABL_PROP_SPECIES_SENSIBLE_ENTHALPY:
+            for (int k = 0; k < ns; k++) out[k] = nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k];
+            return;
+        case ABL_PROP_DENSITY: *out = rho; return;
+    }
+}
+
+template <int DIM>
+__global__ void k_eos_batch(Phys P, int ns, int prop, int64_t n, const double* conserved, const double* T_in, double* out, int* status) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nc = 2 + DIM + ns;
+    const int psz = prop == ABL_PROP_SPECIES_SENSIBLE_ENTHALPY ? ns : 1;
+    double u[2 + 3 + 64];
+    for (int k = 0; k < nc; k++) u[k] = conserved[i * nc + k];
+    bool ok = true;
+    eos_property<DIM>(P, ns, prop, u, T_in != nullptr, T_in ? T_in[i] : 0.0, out + i * psz, &ok);
+    if (!ok) atomicOr(status, kStatusEos);
+}
+
+int status_to_code(int bits) {
+    if (bits & kStatusNaN) return ABL_ERR_NAN;
+    if (bits & kStatusEos) return ABL_ERR_EOS_NOT_CONVERGED;
+    if (bits & kStatusRiemann) return ABL_ERR_RIEMANN_NOT_CONVERGED;
+    return ABL_OK;
+}
+
+}  // namespace
+
+// =================================================================================================
+extern "C" {
+
+const char* abl_last_error_string(void) { return g_last_error.c_str(); }
+
+int abl_version(void) { return 1; }
+
+int abl_device_count(int* count) {
+    return guarded([&] {
+        if (!count) throw std::invalid_argument("count is NULL");
+        int n = 0;
+        cudaError_t e = cudaGetDeviceCount(&n);
+        if (e != cudaSuccess) {
+            *count = 0;
+            throw AblError(ABL_ERR_NO_DEVICE, std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+        }
+        *count = n;
+    });
+}
+
+int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, int device, abl_fv** out) {
+    return guarded([&] {
+        if (!out) throw std::invalid_argument("out is NULL");
+        *out = nullptr;
+        validate_physics(physics);
+        if (!mesh) throw std::invalid_argument("mesh descriptor is NULL");
+        if (!rhs_supported(mesh->dim, physics->n_species))
+            throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for dim " + std::to_string(mesh->dim) + " with " +
+                                                    std::to_string(physics->n_species) + " species");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw AblError(ABL_ERR_NO_DEVICE, "no CUDA device visible");
+        if (device < 0 || device >= ndev) throw std::invalid_argument("device index out of range");
+        ABL_CUDA(cudaSetDevice(device));
+        std::unique_ptr<abl_fv> fv(new abl_fv);
+        fv->device = device;
+        fv->phys = make_phys(physics);
+        const bool lsq = physics->reconstruction == ABL_RECON_LEASTSQUARES;
+        const bool dif = (physics->diffusion || (physics->species_diffusion && physics->n_species > 0)) && physics->transport != ABL_TRANSPORT_NONE;
+        HostMesh h = build_host_mesh(mesh, lsq, dif);
+        fv->dim = h.dim;
+        fv->ns = physics->n_species;
+        fv->nc = 2 + h.dim + fv->ns;
+        fv->naux = 1 + h.dim + fv->ns;
+        fv->n_cells = h.n_cells;
+        fv->n_faces = h.n_faces;
+        fv->n_flux_faces = (int)h.flux_faces.size();
+        fv->need_state_grad = lsq;
+        fv->need_aux_grad = dif;
+        fv->need_aux = true;
+        upload_species(physics, fv->phys, fv->nasa7, fv->mw, fv->inv_mw, fv->href);
+
+        fv->face_cells.upload(reinterpret_cast<const int2*>(h.face_cells.data()), h.n_faces);
+        fv->kind.upload(h.kind.data(), h.kind.size());
+        fv->cone_ptr.upload(h.cone_ptr.data(), h.cone_ptr.size());
+        fv->cone_face.upload(h.cone_face.data(), h.cone_face.size());
+        fv->cone_nbr.upload(h.cone_nbr.data(), h.cone_nbr.size());
+        fv->cone_side.upload(h.cone_side.data(), h.cone_side.size());
+        fv->face_boundary.upload(h.face_boundary.data(), h.face_boundary.size());
+        fv->flux_faces.upload(h.flux_faces.data(), h.flux_faces.size());
+        fv->normal.upload(mesh->face_normal, 3 * (size_t)h.n_faces);
+        fv->fdx.upload(h.fdx.data(), h.fdx.size());
+        fv->vol.upload(mesh->cell_volume, h.n_cells);
+        if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
+        if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
+
+        fv->aux.alloc((size_t)fv->n_cells * fv->naux);
+        {
+            std::vector<double> a0((size_t)fv->n_cells * fv->naux, 0.0);
+            for (int c = 0; c < fv->n_cells; c++) a0[(size_t)c * fv->naux] = 300.0;  // temperature guess (TChem::TemperatureFunction uses 300 K)
+            ABL_CUDA(cudaMemcpy(fv->aux.p, a0.data(), a0.size() * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        fv->fflux.alloc((size_t)fv->n_faces * fv->nc);
+        if (lsq) {
+            fv->grad64.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
+            fv->grad32.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
+        }
+        if (dif) {
+            fv->agrad64.alloc((size_t)fv->n_cells * fv->naux * fv->dim);
+            fv->agrad32.alloc((size_t)fv->n_cells * fv->naux * fv->dim);
+        }
+        fv->status.alloc(1);
+        fv->status.zero();
+
+        DevMesh& M = fv->mesh;
+        M.dim = fv->dim;
+        M.n_cells = fv->n_cells;
+        M.n_faces = fv->n_faces;
+        M.n_flux_faces = fv->n_flux_faces;
+        M.face_cells = fv->face_cells.p;
+        M.kind = fv->kind.p;
+        M.cone_ptr = fv->cone_ptr.p;
+        M.cone_face = fv->cone_face.p;
+        M.cone_nbr = fv->cone_nbr.p;
+        M.cone_side = fv->cone_side.p;
+        M.face_boundary = fv->face_boundary.p;
+        M.flux_faces = fv->flux_faces.p;
+        M.normal = fv->normal.p;
+        M.fdx = fv->fdx.p;
+        M.vol = fv->vol.p;
+        M.cgrad = fv->cgrad.p;
+        M.fgrad = fv->fgrad.p;
+        ABL_CUDA(cudaDeviceSynchronize());
+        *out = fv.release();
+    });
+}
+
+int abl_fv_destroy(abl_fv* fv) {
+    if (!fv) return ABL_OK;
+    cudaSetDevice(fv->device);
+    delete fv;
+    return ABL_OK;
+}
+
+int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells, int32_t* n_faces) {
+    if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (nc) *nc = fv->nc;
+    if (naux) *naux = fv->naux;
+    if (n_cells) *n_cells = fv->n_cells;
+    if (n_faces) *n_faces = fv->n_faces;
+    return ABL_OK;
+}
+
+int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int precision, void* stream) {
+    (void)time;
+    return guarded([&] {
+        if (!fv || !U_dev || !F_dev) throw std::invalid_argument("abl_fv_rhs: NULL argument");
+        if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        dispatch_rhs(fv, U_dev, F_dev, precision, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision) {
+    return guarded([&] {
+        if (!fv || !U_host || !F_host) throw std::invalid_argument("abl_fv_rhs_host: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->hU.n != n) fv->hU.alloc(n);
+        if (fv->hF.n != n) fv->hF.alloc(n);
+        ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        ABL_CUDA(cudaMemcpy(fv->hF.p, F_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision, nullptr);
+        if (rc != ABL_OK) throw AblError(rc, g_last_error);
+        ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int abl_fv_get_aux(abl_fv* fv, double* aux_host) {
+    return guarded([&] {
+        if (!fv || !aux_host) throw std::invalid_argument("NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_CUDA(cudaMemcpy(aux_host, fv->aux.p, fv->aux.n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int abl_fv_set_aux(abl_fv* fv, const double* aux_host) {
+    return guarded([&] {
+        if (!fv || !aux_host) throw std::invalid_argument("NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_CUDA(cudaMemcpy(fv->aux.p, aux_host, fv->aux.n * sizeof(double), cudaMemcpyHostToDevice));
+    });
+}
+
+int abl_fv_status(abl_fv* fv) {
+    if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
+    int bits = 0;
+    int rc = guarded([&] {
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_CUDA(cudaMemcpy(&bits, fv->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        fv->status.zero();
+    });
+    if (rc != ABL_OK) return rc;
+    int code = status_to_code(bits);
+    if (code != ABL_OK) g_last_error = "device status word " + std::to_string(bits);
+    return code;
+}
+
+int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches) {
+    if (!fv || !launches) return fail(ABL_ERR_INVALID_ARGUMENT, "NULL argument");
+    (void)precision;
+    int n = 1;  // gather
+    if (fv->need_aux) n++;
+    if (fv->need_state_grad || fv->need_aux_grad) n++;
+    if (fv->n_flux_faces > 0) n++;
+    *launches = n;
+    return ABL_OK;
+}
+
+int abl_flux_calculator_batch(int kind, double minf, double pgs_alpha, double gamma, int64_t n, const double* uL, const double* aL,
+                              const double* rhoL, const double* pL, const double* uR, const double* aR, const double* rhoR,
+                              const double* pR, double* mass_flux, double* p12, int32_t* direction) {
+    return guarded([&] {
+        if (n < 0 || (n > 0 && (!uL || !aL || !rhoL || !pL || !uR || !aR || !rhoR || !pR || !mass_flux || !direction)))
+            throw std::invalid_argument("abl_flux_calculator_batch: NULL argument");
+        if (kind < ABL_FLUX_OFF || kind > ABL_FLUX_RIEMANN) throw std::invalid_argument("unknown flux calculator");
+        if (n == 0) return;
+        Phys P{};
+        P.flux = kind;
+        P.minf = minf;
+        P.alpha = pgs_alpha > 0 ? pgs_alpha : 1.0;
+        P.gamma = gamma;
+        DevBuf<double> in, outd;
+        DevBuf<int32_t> dir;
+        DevBuf<int> st;
+        in.alloc(8 * (size_t)n);
+        const double* src[8] = {uL, aL, rhoL, pL, uR, aR, rhoR, pR};
+        for (int j = 0; j < 8; j++) ABL_CUDA(cudaMemcpy(in.p + j * n, src[j], n * sizeof(double), cudaMemcpyHostToDevice));
+        outd.alloc(2 * (size_t)n);
+        dir.alloc(n);
+        st.alloc(1);
+        st.zero();
+        k_flux_batch<<<blocks_for(n, 128), 128>>>(P, n, in.p, in.p + n, in.p + 2 * n, in.p + 3 * n, in.p + 4 * n, in.p + 5 * n, in.p + 6 * n,
+                                                  in.p + 7 * n, outd.p, p12 ? outd.p + n : nullptr, dir.p, st.p);
+        check_launch();
+        ABL_CUDA(cudaMemcpy(mass_flux, outd.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (p12) ABL_CUDA(cudaMemcpy(p12, outd.p + n, n * sizeof(double), cudaMemcpyDeviceToHost));
+        ABL_CUDA(cudaMemcpy(direction, dir.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        int bits = 0;
+        ABL_CUDA(cudaMemcpy(&bits, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (bits & kStatusRiemann) throw AblError(ABL_ERR_RIEMANN_NOT_CONVERGED, "Can't find pstar; Iteration not converging");
+    });
+}
+
+int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved, const double* T_in, double* out) {
+    return guarded([&] {
+        validate_physics(physics);
+        if (dim < 1 || dim > 3) throw std::invalid_argument("dim must be 1, 2 or 3");
+        if (property < ABL_PROP_PRESSURE || property > ABL_PROP_DENSITY) throw std::invalid_argument("unknown property");
+        if (n < 0 || (n > 0 && (!conserved || !out))) throw std::invalid_argument("NULL argument");
+        if (n == 0) return;
+        Phys P = make_phys(physics);
+        DevBuf<double> nasa7, mw, inv_mw, href;
+        upload_species(physics, P, nasa7, mw, inv_mw, href);
+        const int ns = physics->n_species;
+        const int nc = 2 + dim + ns;
+        const int psz = property == ABL_PROP_SPECIES_SENSIBLE_ENTHALPY ? ns : 1;
+        DevBuf<double> u, t, o;
+        DevBuf<int> st;
+        u.upload(conserved, (size_t)n * nc);
+        if (T_in) t.upload(T_in, n);
+        o.alloc((size_t)n * (psz > 0 ? psz : 1));
+        st.alloc(1);
+        st.zero();
+        const unsigned nb = blocks_for(n, 128);
+        switch (dim) {
+            case 1: k_eos_batch<1><<<nb, 128>>>(P, ns, property, n, u.p, T_in ? t.p : nullptr, o.p, st.p); break;
+            case 2: k_eos_batch<2><<<nb, 128>>>(P, ns, property, n, u.p, T_in ? t.p : nullptr, o.p, st.p); break;
+            default: k_eos_batch<3><<<nb, 128>>>(P, ns, property, n, u.p, T_in ? t.p : nullptr, o.p, st.p); break;
+        }
+        check_launch();
+        if (psz > 0) ABL_CUDA(cudaMemcpy(out, o.p, (size_t)n * psz * sizeof(double), cudaMemcpyDeviceToHost));
+        int bits = 0;
+        ABL_CUDA(cudaMemcpy(&bits, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (bits & kStatusEos) throw AblError(ABL_ERR_EOS_NOT_CONVERGED, "temperature iteration did not converge");
+    });
+}
+
+}  // extern "C"

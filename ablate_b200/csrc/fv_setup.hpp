@@ -1,0 +1,213 @@
+// fv_setup.hpp -- host-side, one-time preparation of a rank's local mesh for the device:
+// cell cones, face classes and the least-squares weights, built from the geometry DMPlex supplies.
+//
+// Least-squares weights restate, from the geometry alone:
+//   BuildGradientReconstruction_Internal   src/finiteVolume/cellInterpolant.cpp:641-715
+//     (fg->grad[side]: pseudo-inverse of each cell's neighbour offsets over its non-boundary faces)
+//   LeastSquaresAverage::ComputeNeighborCellStencil  src/finiteVolume/stencils/leastSquaresAverage.cpp:71-148
+//     (per-cell gradient operator over every two-sided face, used for face gradients of aux fields)
+// The pseudo-inverse is computed by Householder QR of the offset matrix (full column rank) or by the
+// minimum-norm formula B^T (B B^T)^-1 (fewer offsets than dimensions: a boundary ghost cell).
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ablate_fv.h"
+
+namespace abl {
+
+struct HostMesh {
+    int dim = 0, n_cells = 0, n_faces = 0;
+    std::vector<int32_t> face_cells;     // [nf][2]
+    std::vector<uint8_t> kind;           // [nc]
+    std::vector<int32_t> cone_ptr;       // [nc+1]
+    std::vector<int32_t> cone_face;      // faces of each cell, ascending
+    std::vector<int32_t> cone_nbr;       // neighbour across that face
+    std::vector<uint8_t> cone_side;      // 0: the cell is the face's left cell
+    std::vector<uint8_t> face_boundary;  // a boundary ghost cell is on one side
+    std::vector<int32_t> flux_faces;     // faces with at least one owned cell
+    std::vector<double> cgrad;           // [nf][2][3] cell-interpolant LSQ weights
+    std::vector<double> fgrad;           // [nf][2][3] face-interpolant per-cell stencil weights
+    std::vector<double> fdx;             // [nf][2][3] face centroid minus side-s cell centroid, in that cell's frame
+};
+
+// Pseudo-inverse of B (n x dim, row-major) returned as W (n x dim) with W[i][:] = pinv(B)[:, i].
+inline void lsq_pinv(int n, int dim, const double* B, double* W) {
+    if (n >= dim) {
+        // Householder QR: B = Q R, pinv(B) = R^-1 Q^T
+        std::vector<double> A(B, B + (size_t)n * dim);  // row-major n x dim
+        std::vector<double> vs((size_t)dim * n, 0.0);
+        std::vector<double> beta(dim, 0.0);
+        for (int j = 0; j < dim; j++) {
+            double norm = 0;
+            for (int i = j; i < n; i++) norm += A[i * dim + j] * A[i * dim + j];
+            norm = std::sqrt(norm);
+            if (norm == 0.0) throw std::runtime_error("rank-deficient least-squares stencil");
+            double alpha = A[j * dim + j] > 0 ? -norm : norm;
+            double* v = &vs[(size_t)j * n];
+            for (int i = 0; i < n; i++) v[i] = 0;
+            v[j] = A[j * dim + j] - alpha;
+            for (int i = j + 1; i < n; i++) v[i] = A[i * dim + j];
+            double vv = 0;
+            for (int i = j; i < n; i++) vv += v[i] * v[i];
+            beta[j] = vv > 0 ? 2.0 / vv : 0.0;
+            for (int k = j; k < dim; k++) {
+                double s = 0;
+                for (int i = j; i < n; i++) s += v[i] * A[i * dim + k];
+                s *= beta[j];
+                for (int i = j; i < n; i++) A[i * dim + k] -= s * v[i];
+            }
+        }
+        // columns of pinv: solve R x = (Q^T e_i)[0:dim] for each i
+        std::vector<double> q(n);
+        for (int i = 0; i < n; i++) {
+            for (int r = 0; r < n; r++) q[r] = (r == i) ? 1.0 : 0.0;
+            for (int j = 0; j < dim; j++) {
+                const double* v = &vs[(size_t)j * n];
+                double s = 0;
+                for (int r = j; r < n; r++) s += v[r] * q[r];
+                s *= beta[j];
+                for (int r = j; r < n; r++) q[r] -= s * v[r];
+            }
+            double x[3];
+            for (int j = dim - 1; j >= 0; j--) {
+                double s = q[j];
+                for (int k = j + 1; k < dim; k++) s -= A[j * dim + k] * x[k];
+                x[j] = s / A[j * dim + j];
+            }
+            for (int j = 0; j < dim; j++) W[i * dim + j] = x[j];
+        }
+    } else {
+        // minimum norm: pinv(B) = B^T (B B^T)^-1, n < dim (n = 1 or 2)
+        double G[2][2] = {{0, 0}, {0, 0}};
+        for (int a = 0; a < n; a++)
+            for (int b = 0; b < n; b++)
+                for (int d = 0; d < dim; d++) G[a][b] += B[a * dim + d] * B[b * dim + d];
+        double Gi[2][2];
+        if (n == 1) {
+            Gi[0][0] = 1.0 / G[0][0];
+        } else {
+            double det = G[0][0] * G[1][1] - G[0][1] * G[1][0];
+            Gi[0][0] = G[1][1] / det;
+            Gi[1][1] = G[0][0] / det;
+            Gi[0][1] = -G[0][1] / det;
+            Gi[1][0] = -G[1][0] / det;
+        }
+        for (int i = 0; i < n; i++)
+            for (int d = 0; d < dim; d++) {
+                double s = 0;
+                for (int a = 0; a < n; a++) s += B[a * dim + d] * Gi[a][i];
+                W[i * dim + d] = s;
+            }
+    }
+}
+
+inline HostMesh build_host_mesh(const abl_mesh_desc* m, bool need_cgrad, bool need_fgrad) {
+    HostMesh h;
+    if (!m || m->dim < 1 || m->dim > 3 || m->n_cells <= 0 || m->n_faces < 0 || !m->face_cells || !m->face_normal || !m->face_centroid ||
+        !m->cell_centroid || !m->cell_volume)
+        throw std::invalid_argument("invalid mesh descriptor");
+    h.dim = m->dim;
+    h.n_cells = m->n_cells;
+    h.n_faces = m->n_faces;
+    const int nc = h.n_cells, nf = h.n_faces, dim = h.dim;
+    h.face_cells.assign(m->face_cells, m->face_cells + 2 * (size_t)nf);
+    h.kind.assign(nc, ABL_CELL_OWNED);
+    if (m->cell_kind)
+        for (int c = 0; c < nc; c++) {
+            if (m->cell_kind[c] > ABL_CELL_HALO_OUTER) throw std::invalid_argument("invalid cell kind");
+            h.kind[c] = m->cell_kind[c];
+        }
+    for (int c = 0; c < nc; c++)
+        if (!(m->cell_volume[c] > 0.0)) throw std::invalid_argument("cell volume must be positive (cell " + std::to_string(c) + ")");
+    h.cone_ptr.assign(nc + 1, 0);
+    for (int f = 0; f < nf; f++) {
+        int a = h.face_cells[2 * f], b = h.face_cells[2 * f + 1];
+        if (a < 0 || a >= nc || b < 0 || b >= nc || a == b) throw std::invalid_argument("face " + std::to_string(f) + " has an invalid support");
+        h.cone_ptr[a + 1]++;
+        h.cone_ptr[b + 1]++;
+    }
+    for (int c = 0; c < nc; c++) h.cone_ptr[c + 1] += h.cone_ptr[c];
+    const size_t ncone = h.cone_ptr[nc];
+    h.cone_face.resize(ncone);
+    h.cone_nbr.resize(ncone);
+    h.cone_side.resize(ncone);
+    std::vector<int32_t> fill(h.cone_ptr.begin(), h.cone_ptr.end() - 1);
+    for (int f = 0; f < nf; f++)
+        for (int s = 0; s < 2; s++) {
+            int c = h.face_cells[2 * f + s];
+            int i = fill[c]++;
+            h.cone_face[i] = f;
+            h.cone_nbr[i] = h.face_cells[2 * f + (1 - s)];
+            h.cone_side[i] = (uint8_t)s;
+        }
+    for (int c = 0; c < nc; c++)
+        if (h.kind[c] == ABL_CELL_BOUNDARY && h.cone_ptr[c + 1] - h.cone_ptr[c] != 1)
+            throw std::invalid_argument("boundary ghost cell " + std::to_string(c) + " must have exactly one face");
+    h.face_boundary.assign(nf, 0);
+    for (int f = 0; f < nf; f++) {
+        uint8_t ka = h.kind[h.face_cells[2 * f]], kb = h.kind[h.face_cells[2 * f + 1]];
+        h.face_boundary[f] = (ka == ABL_CELL_BOUNDARY || kb == ABL_CELL_BOUNDARY);
+        if (ka == ABL_CELL_OWNED || kb == ABL_CELL_OWNED) h.flux_faces.push_back(f);
+    }
+    // offset from each side's cell centroid to the face centroid, periodic images resolved
+    h.fdx.assign((size_t)nf * 6, 0.0);
+    for (int f = 0; f < nf; f++) {
+        const int a = h.face_cells[2 * f], b = h.face_cells[2 * f + 1];
+        for (int d = 0; d < dim; d++) {
+            const double sh = m->face_shift ? m->face_shift[3 * (size_t)f + d] : 0.0;
+            h.fdx[6 * (size_t)f + d] = m->face_centroid[3 * (size_t)f + d] - m->cell_centroid[3 * (size_t)a + d];
+            h.fdx[6 * (size_t)f + 3 + d] = (m->face_centroid[3 * (size_t)f + d] - sh) - m->cell_centroid[3 * (size_t)b + d];
+        }
+    }
+    // neighbour offset x_n - x_c across cone entry i (periodic images resolved)
+    auto nbr_dx = [&](int c, int i, int d) {
+        const int f = h.cone_face[i];
+        const int n = h.cone_nbr[i];
+        const double sh = m->face_shift ? m->face_shift[3 * (size_t)f + d] : 0.0;
+        const double xn = m->cell_centroid[3 * (size_t)n + d] + (h.cone_side[i] == 0 ? sh : -sh);
+        return xn - m->cell_centroid[3 * (size_t)c + d];
+    };
+    std::vector<double> B, W;
+    if (need_cgrad) {
+        h.cgrad.assign((size_t)nf * 6, 0.0);
+        for (int c = 0; c < nc; c++) {
+            if (h.kind[c] != ABL_CELL_OWNED && h.kind[c] != ABL_CELL_HALO) continue;
+            B.clear();
+            std::vector<size_t> slots;
+            for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                if (h.face_boundary[h.cone_face[i]]) continue;
+                for (int d = 0; d < dim; d++) B.push_back(nbr_dx(c, i, d));
+                slots.push_back((size_t)h.cone_face[i] * 6 + 3 * h.cone_side[i]);
+            }
+            if (slots.empty()) throw std::invalid_argument("isolated cell " + std::to_string(c) + " has no neighbours");
+            W.assign(B.size(), 0.0);
+            lsq_pinv((int)slots.size(), dim, B.data(), W.data());
+            for (size_t i = 0; i < slots.size(); i++)
+                for (int d = 0; d < dim; d++) h.cgrad[slots[i] + d] = W[i * dim + d];
+        }
+    }
+    if (need_fgrad) {
+        h.fgrad.assign((size_t)nf * 6, 0.0);
+        for (int c = 0; c < nc; c++) {
+            if (h.kind[c] == ABL_CELL_HALO_OUTER) continue;
+            B.clear();
+            std::vector<size_t> slots;
+            for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                for (int d = 0; d < dim; d++) B.push_back(nbr_dx(c, i, d));
+                slots.push_back((size_t)h.cone_face[i] * 6 + 3 * h.cone_side[i]);
+            }
+            if (slots.empty()) continue;
+            W.assign(B.size(), 0.0);
+            lsq_pinv((int)slots.size(), dim, B.data(), W.data());
+            for (size_t i = 0; i < slots.size(); i++)
+                for (int d = 0; d < dim; d++) h.fgrad[slots[i] + d] = W[i * dim + d];
+        }
+    }
+    return h;
+}
+
+}  // namespace abl

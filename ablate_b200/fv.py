@@ -1,0 +1,370 @@
+"""Host-side mirror of ABLATE's FV process interfaces, driving the B200 backend through its C ABI.
+
+The objects here carry the same names and constructor arguments as the reference classes they stand
+for, and ``FiniteVolumeSolver`` wires them the way ``Process::Setup`` / ``RegisterRHSFunction`` do:
+
+  eos.PerfectGas(parameters, species)              src/eos/perfectGas.cpp:4-7 (gamma 1.4, Rgas 287 defaults)
+  eos.TChem(species thermo)                        src/eos/tChem.cpp (NASA-7 thermodynamics only)
+  fluxCalculator.{Ausm, AusmpUp, Riemann, AverageFlux, OffFlux}
+                                                   src/finiteVolume/fluxCalculator/*.cpp
+  transport.{Constant, Sutherland, ConstantLewis}  src/eos/transport/{constant,sutherland}.cpp
+  processes.{NavierStokesTransport, SpeciesTransport}
+                                                   src/finiteVolume/processes/{navierStokesTransport,speciesTransport}.cpp
+  FiniteVolumeSolver.ComputeRHSFunction            src/finiteVolume/finiteVolumeSolver.cpp:233-291
+
+Every numeric path goes to the sm_100a kernels of ``lib/libablate_fv.so``; there is no CPU
+implementation in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib as L
+
+
+# ---------------------------------------------------------------------------------------------
+# eos
+# ---------------------------------------------------------------------------------------------
+class PerfectGas:
+    """ablate::eos::PerfectGas (src/eos/perfectGas.cpp:4-7)."""
+
+    def __init__(self, parameters: dict | None = None, species: Sequence[str] = ()):
+        parameters = parameters or {}
+        self.gamma = float(parameters.get("gamma", 1.4))
+        self.rGas = float(parameters.get("Rgas", 287.0))
+        self.species = list(species)
+
+    def GetSpecificHeatRatio(self):
+        return self.gamma
+
+    def GetGasConstant(self):
+        return self.rGas
+
+    def GetSpeciesVariables(self):
+        return list(self.species)
+
+    def _fill(self, p: L.PhysicsDesc, keep: list):
+        p.eos = L.EOS_PERFECT_GAS
+        p.gamma = self.gamma
+        p.r_gas = self.rGas
+
+
+# atomic weights (kg/kmol) used to form species molar masses from their elemental composition
+ATOMIC_WEIGHTS = {"H": 1.00797, "O": 15.9994, "C": 12.01115, "N": 14.0067, "AR": 39.948, "Ar": 39.948, "HE": 4.0026, "He": 4.0026}
+
+
+class TChem:
+    """NASA-7 mixture EOS (the thermodynamics of ablate::eos::TChem, src/eos/tChem.cpp).
+
+    ``species`` is a list of dicts with keys name, composition (element -> count), T_ranges
+    [T_low, T_mid, T_high], low (7 coefficients), high (7 coefficients), as in a Cantera YAML file.
+    """
+
+    def __init__(self, species: list[dict], atomic_weights: dict | None = None):
+        aw = atomic_weights or ATOMIC_WEIGHTS
+        self.names = [s["name"] for s in species]
+        ns = len(species)
+        self.nasa7 = np.zeros((ns, 15))
+        self.mw = np.zeros(ns)
+        for k, s in enumerate(species):
+            self.nasa7[k, 0] = s["T_ranges"][1]
+            self.nasa7[k, 1:8] = s["low"]
+            self.nasa7[k, 8:15] = s["high"]
+            self.mw[k] = sum(aw[el] * n for el, n in s["composition"].items())
+
+    @classmethod
+    def from_yaml(cls, path, atomic_weights: dict | None = None):
+        """Read NASA-7 species from a Cantera-format YAML mechanism (YAML 1.1 booleans disabled so that
+        species such as NO and elements such as N stay strings)."""
+        import yaml
+
+        class Loader(yaml.SafeLoader):
+            pass
+
+        Loader.yaml_implicit_resolvers = {k: [(t, r) for t, r in v if t != "tag:yaml.org,2002:bool"]
+                                          for k, v in yaml.SafeLoader.yaml_implicit_resolvers.items()}
+        doc = yaml.load(open(path).read(), Loader=Loader)
+        species = []
+        for sp in doc["species"]:
+            th = sp["thermo"]
+            species.append({"name": sp["name"], "composition": sp["composition"], "T_ranges": th["temperature-ranges"],
+                            "low": th["data"][0], "high": th["data"][1]})
+        return cls(species, atomic_weights)
+
+    def GetSpeciesVariables(self):
+        return list(self.names)
+
+    def _fill(self, p: L.PhysicsDesc, keep: list):
+        p.eos = L.EOS_NASA7
+        a = np.ascontiguousarray(self.nasa7)
+        m = np.ascontiguousarray(self.mw)
+        keep += [a, m]
+        p.nasa7 = L.dptr(a)
+        p.mw = L.dptr(m)
+        p.gamma = 1.4
+        p.r_gas = 287.0
+
+
+# ---------------------------------------------------------------------------------------------
+# flux calculators
+# ---------------------------------------------------------------------------------------------
+class _Flux:
+    kind = L.FLUX_OFF
+
+    def _params(self):
+        return 0.0, 1.0, 1.4
+
+    def GetFluxCalculatorFunction(self):
+        """Vectorised FluxCalculatorFunction evaluated on the device: (massFlux, p12, direction) arrays."""
+        kind = self.kind
+        minf, alpha, gamma = self._params()
+
+        def fn(uL, aL, rhoL, pL, uR, aR, rhoR, pR):
+            arrs = [np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64) for x in (uL, aL, rhoL, pL, uR, aR, rhoR, pR)]
+            n = arrs[0].size
+            mf, p12 = np.zeros(n), np.zeros(n)
+            d = np.zeros(n, np.int32)
+            L.check(L.lib.abl_flux_calculator_batch(kind, minf, alpha, gamma, n, *[L.dptr(a) for a in arrs], L.dptr(mf), L.dptr(p12),
+                                                    L.iptr(d)), "flux calculator")
+            return mf, p12, d
+
+        return fn
+
+
+class Ausm(_Flux):
+    kind = L.FLUX_AUSM
+
+
+class AusmpUp(_Flux):
+    """AusmpUp(mInf, pgs): pgs may be a PressureGradientScaling-like object with GetAlpha() or a number."""
+    kind = L.FLUX_AUSMPUP
+
+    def __init__(self, mInf: float = 0.0, pgs=None):
+        self.mInf = float(mInf)
+        self.pgs = pgs
+
+    def _alpha(self):
+        if self.pgs is None:
+            return 1.0
+        return float(self.pgs.GetAlpha() if hasattr(self.pgs, "GetAlpha") else self.pgs)
+
+    def _params(self):
+        return self.mInf, self._alpha(), 1.4
+
+
+class Riemann(_Flux):
+    kind = L.FLUX_RIEMANN
+
+    def __init__(self, eos):
+        if not isinstance(eos, PerfectGas):
+            raise ValueError("Riemann only accepts EOS of type eos::PerfectGas")
+        self.gamma = eos.GetSpecificHeatRatio()
+
+    def _params(self):
+        return 0.0, 1.0, self.gamma
+
+
+class AverageFlux(_Flux):
+    kind = L.FLUX_AVERAGE
+
+
+class OffFlux(_Flux):
+    kind = L.FLUX_OFF
+
+
+class PressureGradientScaling:
+    """Only the alpha used by AusmpUp (src/finiteVolume/processes/pressureGradientScaling.hpp:84)."""
+
+    def __init__(self, eos=None, alphaInit: float = 1.0, *args):
+        self.alpha = float(alphaInit)
+
+    def GetAlpha(self):
+        return self.alpha
+
+
+# ---------------------------------------------------------------------------------------------
+# transport
+# ---------------------------------------------------------------------------------------------
+class Constant:
+    def __init__(self, k: float = 0.0, mu: float = 0.0, diff: float = 0.0):
+        self.k, self.mu, self.diff = float(k), float(mu), float(diff)
+
+    def _fill(self, p):
+        p.transport = L.TRANSPORT_CONSTANT
+        p.k, p.mu, p.diff = self.k, self.mu, self.diff
+
+
+class Sutherland:
+    def __init__(self, eos=None):
+        self.eos = eos
+
+    def _fill(self, p):
+        p.transport = L.TRANSPORT_SUTHERLAND
+
+
+class ConstantLewis:
+    """Constant viscosity, k = mu cp / Pr, species diffusivity D = k / (rho cp Le). No reference counterpart."""
+
+    def __init__(self, mu: float, prandtl: float = 0.72, lewis: float = 1.0):
+        self.mu, self.prandtl, self.lewis = float(mu), float(prandtl), float(lewis)
+
+    def _fill(self, p):
+        p.transport = L.TRANSPORT_CONSTANT_LEWIS
+        p.mu, p.k, p.diff = self.mu, self.prandtl, self.lewis
+
+
+# ---------------------------------------------------------------------------------------------
+# processes
+# ---------------------------------------------------------------------------------------------
+class NavierStokesTransport:
+    """src/finiteVolume/processes/navierStokesTransport.cpp:10-97"""
+
+    def __init__(self, parameters: dict | None, eos, fluxCalculator=None, transport=None, pgs=None):
+        self.parameters = parameters or {}
+        self.eos, self.fluxCalculator, self.transport = eos, fluxCalculator, transport
+
+    def Setup(self, flow: "FiniteVolumeSolver"):
+        if self.fluxCalculator is not None:
+            flow.RegisterRHSFunction("NavierStokesTransport::AdvectionFlux", self.fluxCalculator)
+        if self.transport is not None:
+            flow.RegisterRHSFunction("NavierStokesTransport::DiffusionFlux", self.transport)
+
+
+class SpeciesTransport:
+    """src/finiteVolume/processes/speciesTransport.cpp:7-96"""
+
+    def __init__(self, eos, fluxCalculator=None, transport=None, parameters: dict | None = None):
+        self.eos, self.fluxCalculator, self.transport = eos, fluxCalculator, transport
+
+    def Setup(self, flow: "FiniteVolumeSolver"):
+        if not self.eos.GetSpeciesVariables():
+            return
+        if self.fluxCalculator is not None:
+            flow.RegisterRHSFunction("SpeciesTransport::AdvectionFlux", self.fluxCalculator)
+        if self.transport is not None:
+            flow.RegisterRHSFunction("SpeciesTransport::DiffusionSpeciesFlux", self.transport)
+
+
+# ---------------------------------------------------------------------------------------------
+# solver
+# ---------------------------------------------------------------------------------------------
+LIMITERS = {"none": L.LIMITER_NONE, "zero": L.LIMITER_ZERO, "minmod": L.LIMITER_MINMOD, "vanleer": L.LIMITER_VANLEER,
+            "vanalbada": L.LIMITER_VANALBADA, "sin": L.LIMITER_SIN}
+
+
+def make_physics(eos, processes, petscfv_type: str = "upwind", limiter: str = "none", maxLimGrad: float = 1e10):
+    """Build the abl_physics_desc the processes register. Returns (desc, keep-alive list)."""
+    p = L.PhysicsDesc()
+    keep: list = []
+    eos._fill(p, keep)
+    p.n_species = len(eos.GetSpeciesVariables())
+    p.pgs_alpha = 1.0
+    p.max_lim_grad = maxLimGrad
+    p.reconstruction = L.RECON_LEASTSQUARES if petscfv_type == "leastsquares" else L.RECON_UPWIND
+    p.limiter = LIMITERS[limiter]
+    p.transport = L.TRANSPORT_NONE
+    flux = None
+    for proc in processes:
+        if isinstance(proc, NavierStokesTransport):
+            if proc.fluxCalculator is not None:
+                p.advection = 1
+                flux = proc.fluxCalculator
+            if proc.transport is not None:
+                p.diffusion = 1
+                proc.transport._fill(p)
+        elif isinstance(proc, SpeciesTransport):
+            if not eos.GetSpeciesVariables():
+                continue
+            if proc.fluxCalculator is not None:
+                p.species_advection = 1
+                if flux is not None and type(flux) is not type(proc.fluxCalculator):
+                    raise ValueError("NavierStokesTransport and SpeciesTransport must share one flux calculator type")
+                flux = proc.fluxCalculator
+            if proc.transport is not None:
+                p.species_diffusion = 1
+                proc.transport._fill(p)
+    if flux is not None:
+        p.flux = flux.kind
+        minf, alpha, gamma = flux._params()
+        p.ausmpup_minf = minf
+        p.pgs_alpha = alpha
+    return p, keep
+
+
+class FiniteVolumeSolver:
+    """Owns one abl_fv handle: mesh + geometry + weights resident on one GPU."""
+
+    def __init__(self, mesh, eos, processes, petscfv_type: str = "upwind", limiter: str = "none", maxLimGrad: float = 1e10,
+                 device: int = 0):
+        self.mesh = mesh
+        self.eos = eos
+        self.processes = list(processes)
+        self.registered: list[str] = []
+        for proc in self.processes:
+            proc.Setup(self)
+        self.physics, self._keep = make_physics(eos, self.processes, petscfv_type, limiter, maxLimGrad)
+        desc = mesh.desc()
+        h = C.c_void_p()
+        L.check(L.lib.abl_fv_create(C.byref(desc), C.byref(self.physics), device, C.byref(h)), "abl_fv_create")
+        self.handle = h
+        nc, na, ncell, nf = (C.c_int32() for _ in range(4))
+        L.check(L.lib.abl_fv_sizes(h, C.byref(nc), C.byref(na), C.byref(ncell), C.byref(nf)))
+        self.nc, self.naux, self.n_cells, self.n_faces = nc.value, na.value, ncell.value, nf.value
+
+    def RegisterRHSFunction(self, name: str, obj):
+        self.registered.append(name)
+
+    def ComputeRHSFunction(self, time: float, locX: np.ndarray, locF: np.ndarray, precision: int = L.PRECISION_FP64):
+        """locF += RHS(locX) with host arrays (n_cells, nc)."""
+        assert locX.shape == (self.n_cells, self.nc) and locF.shape == locX.shape
+        x = np.ascontiguousarray(locX, dtype=np.float64)
+        assert locF.dtype == np.float64 and locF.flags.c_contiguous
+        L.check(L.lib.abl_fv_rhs_host(self.handle, time, L.dptr(x), L.dptr(locF), precision), "abl_fv_rhs_host")
+        return locF
+
+    def ComputeRHSDevice(self, time: float, U_ptr: int, F_ptr: int, precision: int = L.PRECISION_FP64, stream: int = 0):
+        """F += RHS(U) with device pointers (e.g. torch tensors' data_ptr()), enqueued on `stream`."""
+        L.check(L.lib.abl_fv_rhs(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(F_ptr), precision, C.c_void_p(stream)), "abl_fv_rhs")
+
+    def GetAux(self) -> np.ndarray:
+        a = np.zeros((self.n_cells, self.naux))
+        L.check(L.lib.abl_fv_get_aux(self.handle, L.dptr(a)))
+        return a
+
+    def SetAux(self, aux: np.ndarray):
+        a = np.ascontiguousarray(aux, dtype=np.float64)
+        L.check(L.lib.abl_fv_set_aux(self.handle, L.dptr(a)))
+
+    def Status(self) -> int:
+        return L.lib.abl_fv_status(self.handle)
+
+    def LaunchCount(self, precision: int = L.PRECISION_FP64) -> int:
+        n = C.c_int32()
+        L.check(L.lib.abl_fv_launch_count(self.handle, precision, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            L.lib.abl_fv_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def eos_property(physics: L.PhysicsDesc, dim: int, prop: int, conserved: np.ndarray, T: np.ndarray | None = None) -> np.ndarray:
+    """Device batch of a ThermodynamicFunction (T is None) or ThermodynamicTemperatureFunction."""
+    conserved = np.ascontiguousarray(conserved, dtype=np.float64)
+    n = conserved.shape[0]
+    ps = physics.n_species if prop == L.PROP_SPECIES_SENSIBLE_ENTHALPY else 1
+    out = np.zeros((n, max(ps, 1)))
+    Ta = None if T is None else np.ascontiguousarray(T, dtype=np.float64)
+    L.check(L.lib.abl_eos_batch(C.byref(physics), dim, prop, n, L.dptr(conserved), L.dptr(Ta), L.dptr(out)), "abl_eos_batch")
+    return out

@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark of the FV right-hand side (FiniteVolumeSolver::ComputeRHSFunction) on B200.
+
+One "step" is one RHS evaluation of the whole synthetic workload with the state resident in HBM.
+Default workload: the 128^3 periodic Navier-Stokes Taylor-Green case (AUSM+up, least squares +
+minmod, constant viscosity), run at FP64 and on the mixed path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tgv3d|sod2d|shear3d]
+
+With --gpus N > 1 it runs under torch.distributed.run, one rank per GPU, each rank holding its own
+copy of the workload (replicas; weak scaling, no data-path collective). Device times come from CUDA
+events around each RHS on the launching stream, L2 flushed between timed steps, max over ranks.
+``--impl reference`` times the CPU restatement of the reference algorithm (the oracle; the reference
+itself needs PETSc/MPI/TChem, absent here) on all host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "FV RHS Mcell-updates/s (FP64 vs mixed @1e-6 rel), HBM GB/s, VJP/RHS cost"
+UNIT = "Mcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "sod2d", "shear3d"])
+    ap.add_argument("--n", type=int, default=0, help="mesh cells per direction (default: the configuration's size)")
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def make_workload(name, n):
+    from ablate_b200 import workloads
+
+    if name == "tgv3d":
+        return workloads.tgv3d(n or 128)
+    if name == "sod2d":
+        return workloads.sod2d(n or 256)
+    return workloads.shear3d(n or 256, 5)
+
+
+def algorithmic_bytes(w):
+    """Compulsory traffic of one RHS: read the FP64 state once, write the residual once, read 1/V per
+    cell; per face read two int32 cell indices and the FP64 area normal."""
+    n_cells = int(w.mesh.n_interior)
+    nc = w.U.shape[1]
+    n_faces = int(w.mesh.n_faces)
+    return n_cells * (2 * nc * 8 + 8) + n_faces * (2 * 4 + w.mesh.dim * 8)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5], parts[6], parts[7], parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def read_traffic(workload: str, precision: str):
+    """DRAM bytes per RHS from the committed ncu summary (profiles/rhs_<workload>_traffic.txt), if any."""
+    p = ROOT / "profiles" / f"rhs_{workload}_traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith(f"{precision}_dram_bytes_per_rhs:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def cpu_baseline(w, phys, seconds):
+    from oracle import oracle as orc
+    from ablate_b200.workloads import initial_aux
+
+    threads = os.cpu_count() or 1
+    R = orc.OracleRHS(w.mesh, phys)
+    aux = initial_aux(w)
+    F = np.zeros_like(w.U)
+    R(w.U, aux, F, threads)  # warm-up
+    times = []
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end or len(times) < 2:
+        F[:] = 0.0
+        t0 = time.perf_counter()
+        R(w.U, aux, F, threads)
+        times.append(time.perf_counter() - t0)
+    R.close()
+    t = statistics.median(times)
+    return {"value": w.mesh.n_interior / t / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"full workload, {len(times)} RHS evaluations (median), oracle restatement with OpenMP over {threads} threads"}, F
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = make_workload(args.workload, args.n)
+    phys, keep = w.physics()
+    from oracle import oracle as orc
+    from ablate_b200.workloads import initial_aux
+
+    threads = os.cpu_count() or 1
+    R = orc.OracleRHS(w.mesh, phys)
+    aux = initial_aux(w)
+    F = np.zeros_like(w.U)
+    for _ in range(args.warmup):
+        R(w.U, aux, F, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        R(w.U, aux, F, threads)
+    t = (time.perf_counter() - t0) / args.steps
+    value = w.mesh.n_interior / t / 1e6
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "n_cells": int(w.mesh.n_interior), "n_faces": int(w.mesh.n_faces), "description": w.description},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"one full RHS per step, {threads} OpenMP threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    from ablate_b200 import _lib as L
+    from ablate_b200.workloads import initial_aux
+
+    w = make_workload(args.workload, args.n)
+    solver = w.solver(device=local)
+    solver.SetAux(initial_aux(w))
+    U = torch.from_numpy(w.U).to(dev)
+    F = torch.zeros_like(U)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream(dev)
+    precisions = {"fp64": [L.PRECISION_FP64], "mixed": [L.PRECISION_MIXED], "both": [L.PRECISION_FP64, L.PRECISION_MIXED]}[args.precision]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def rhs(prec):
+        solver.ComputeRHSDevice(0.0, U.data_ptr(), F.data_ptr(), prec, stream.cuda_stream)
+
+    results = {}
+    clocks = None
+    for prec in precisions:
+        for _ in range(args.warmup):
+            rhs(prec)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        with ClockSampler(local) as cs:
+            for k in range(args.steps):
+                flush.zero_()
+                evs[k][0].record(stream)
+                rhs(prec)
+                evs[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        if clocks is None:
+            clocks = cs.summary()
+        total_ms = sum(a.elapsed_time(b) for a, b in evs)
+        if world > 1:
+            t = torch.tensor([total_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        rc = solver.Status()
+        if rc != L.OK:
+            raise RuntimeError(f"device status {rc} after the timed RHS")
+        results[prec] = total_ms / args.steps
+
+    # accuracy of the mixed path against FP64 on this workload
+    mixed_err = None
+    if L.PRECISION_MIXED in results:
+        F64 = torch.zeros_like(U)
+        F32 = torch.zeros_like(U)
+        solver.ComputeRHSDevice(0.0, U.data_ptr(), F64.data_ptr(), L.PRECISION_FP64, stream.cuda_stream)
+        solver.ComputeRHSDevice(0.0, U.data_ptr(), F32.data_ptr(), L.PRECISION_MIXED, stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        owned = torch.from_numpy(w.mesh.cell_kind == L.CELL_OWNED).to(dev)
+        neul = 2 + w.mesh.dim
+        a, b = F32[owned], F64[owned]
+        mixed_err = {"euler": float((a[:, :neul] - b[:, :neul]).norm() / b[:, :neul].norm())}
+        if a.shape[1] > neul:
+            mixed_err["densityYi"] = float((a[:, neul:] - b[:, neul:]).norm() / b[:, neul:].norm())
+
+    # end to end through the public host API: pinned host buffers, H2D of U and F, RHS, D2H of F
+    head = L.PRECISION_FP64 if L.PRECISION_FP64 in results else precisions[0]
+    Uh = torch.from_numpy(w.U).pin_memory()
+    Fh = torch.zeros_like(Uh).pin_memory()
+    Un, Fn = Uh.numpy(), Fh.numpy()
+    for _ in range(2):
+        solver.ComputeRHSFunction(0.0, Un, Fn, head)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e2e_steps = max(3, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.ComputeRHSFunction(0.0, Un, Fn, head)
+    torch.cuda.synchronize(dev)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    state_bytes = int(w.U.nbytes)
+
+    n_cells = int(w.mesh.n_interior)
+    B = algorithmic_bytes(w)
+    peak, peak_kind = measured_peaks()
+    head_ms = results[head]
+    value = world * n_cells / (head_ms * 1e-3) / 1e6
+    achieved = B / (head_ms * 1e-3) / 1e9
+    launches = solver.LaunchCount(head) * args.steps
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == L.PRECISION_FP64 else "mixed f32/f64", "data": "synthetic",
+        "config": {"workload": w.name, "n_cells": n_cells, "n_faces": int(w.mesh.n_faces), "description": w.description,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MiB write) between timed steps, outside the timed events"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed"),
+                     "algorithmic_bytes_per_rhs": B, "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                     "scope": "whole RHS (all kernels of one abl_fv_rhs call)"},
+        "precisions": {("fp64" if p == L.PRECISION_FP64 else "mixed"): {"ms_per_step": ms, "mcell_per_s": world * n_cells / (ms * 1e-3) / 1e6,
+                                                                          "hbm_gbs": B / (ms * 1e-3) / 1e9}
+                       for p, ms in results.items()},
+        "mixed_rel_err_vs_fp64": mixed_err,
+        "vjp_over_rhs": None,
+        "e2e": {"value": world * n_cells / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 2 * state_bytes,
+                "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,
+                "path": "abl_fv_rhs_host: pinned host U and F copied in, RHS, F copied out, every step"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        phys, keep = w.physics()
+        cb, F_cpu = cpu_baseline(w, phys, args.cpu_seconds)
+        line["cpu_baseline"] = cb
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,209 @@
+/*
+ * ablate_fv.h -- C ABI of the B200 finite-volume right-hand-side backend.
+ *
+ * This library replaces, for one PETSc rank, the discontinuous and continuous flux loops that
+ * ablate::finiteVolume::FiniteVolumeSolver::ComputeRHSFunction runs
+ * (src/finiteVolume/finiteVolumeSolver.cpp:233-291 in ABLATE 0.13.03):
+ *
+ *   CellInterpolant::ComputeRHS        src/finiteVolume/cellInterpolant.cpp:43-140
+ *     ComputeFieldGradients + limiter  src/finiteVolume/cellInterpolant.cpp:282-497
+ *     ComputeFluxSourceTerms           src/finiteVolume/cellInterpolant.cpp:499-639
+ *   FaceInterpolant::ComputeRHS        src/finiteVolume/faceInterpolant.cpp:262-448
+ *   NavierStokesTransport::AdvectionFlux / DiffusionFlux
+ *                                      src/finiteVolume/processes/navierStokesTransport.cpp:99-207, 454-532
+ *   SpeciesTransport::AdvectionFlux / DiffusionSpeciesFlux / DiffusionEnergyFlux
+ *                                      src/finiteVolume/processes/speciesTransport.cpp:112-341
+ *   the aux update run before it       src/solver/cellSolver.cpp:62-135
+ *
+ * Everything crossing this boundary is plain C: pointers, sizes and status codes. No C++ exception
+ * crosses it. Every entry point returns ABL_OK (0) or a negative ABL_ERR_* code; the text of the last
+ * error of the calling thread is returned by abl_last_error_string().
+ *
+ * Data layout (identical to the PETSc local vectors ABLATE hands to its flux functions):
+ *   state     U[n_cells][nc],  nc  = 2 + dim + n_species:  rho, rhoE, rho*u[dim], rho*Y[n_species]
+ *             (the "euler" field then the "densityYi" field, src/finiteVolume/compressibleFlowFields.cpp:12-29)
+ *   residual  F[n_cells][nc], same layout; the backend ADDS into it (locF is zeroed by the caller,
+ *             src/solver/timeStepper.cpp:363) and only touches owned cells.
+ *   aux       A[n_cells][naux], naux = 1 + dim + n_species: T, u[dim], Y[n_species]
+ * All floating point values are IEEE binary64.
+ */
+#ifndef ABLATE_FV_H
+#define ABLATE_FV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------------- */
+#define ABL_OK 0
+#define ABL_ERR_INVALID_ARGUMENT -1 /* bad pointer, size, enum or mesh descriptor                   */
+#define ABL_ERR_CUDA -2             /* a CUDA runtime call failed                                   */
+#define ABL_ERR_NAN -3              /* a NaN or Inf appeared in the residual (device status word)  */
+#define ABL_ERR_EOS_NOT_CONVERGED -4 /* the mixture temperature iteration hit its iteration cap     */
+#define ABL_ERR_RIEMANN_NOT_CONVERGED -5 /* exact Riemann p* iteration failed                       */
+#define ABL_ERR_OUT_OF_MEMORY -6
+#define ABL_ERR_UNSUPPORTED -7      /* configuration not supported by this build                   */
+#define ABL_ERR_NO_DEVICE -8        /* no CUDA device visible                                       */
+
+/* ---- enums ------------------------------------------------------------------------------------ */
+/* fluxCalculator::FluxCalculator implementations (src/finiteVolume/fluxCalculator/) */
+#define ABL_FLUX_OFF 0     /* offFlux.cpp:2-9     */
+#define ABL_FLUX_AVERAGE 1 /* averageFlux.cpp:2-11 */
+#define ABL_FLUX_AUSM 2    /* ausm.cpp:2-43       */
+#define ABL_FLUX_AUSMPUP 3 /* ausmpUp.cpp:5-96    */
+#define ABL_FLUX_RIEMANN 4 /* riemann.cpp:6-36 + riemannSolver.cpp:7-187 */
+
+/* fluxCalculator::Direction (src/finiteVolume/fluxCalculator/fluxCalculator.hpp:12) */
+#define ABL_DIR_NA 0
+#define ABL_DIR_LEFT 1
+#define ABL_DIR_RIGHT 2
+
+/* eos::EOS implementations */
+#define ABL_EOS_PERFECT_GAS 0 /* src/eos/perfectGas.cpp                                    */
+#define ABL_EOS_NASA7 1       /* src/eos/tChem.cpp (TChem NASA-7 thermodynamics, no kinetics) */
+
+/* eos::ThermodynamicProperty (src/eos/eos.hpp:14-24), same order */
+#define ABL_PROP_PRESSURE 0
+#define ABL_PROP_TEMPERATURE 1
+#define ABL_PROP_INTERNAL_SENSIBLE_ENERGY 2
+#define ABL_PROP_SENSIBLE_ENTHALPY 3
+#define ABL_PROP_CV 4
+#define ABL_PROP_CP 5
+#define ABL_PROP_SPEED_OF_SOUND 6
+#define ABL_PROP_SPECIES_SENSIBLE_ENTHALPY 7
+#define ABL_PROP_DENSITY 8
+
+/* eos::transport::TransportModel implementations */
+#define ABL_TRANSPORT_NONE 0
+#define ABL_TRANSPORT_CONSTANT 1       /* src/eos/transport/constant.cpp   */
+#define ABL_TRANSPORT_SUTHERLAND 2     /* src/eos/transport/sutherland.cpp */
+#define ABL_TRANSPORT_CONSTANT_LEWIS 3 /* k = mu*cp/Pr, D = k/(rho*cp*Le); no reference counterpart */
+
+/* PetscFV type of the conserved fields */
+#define ABL_RECON_UPWIND 0        /* PETSCFVUPWIND: first order, no gradients         */
+#define ABL_RECON_LEASTSQUARES 1  /* PETSCFVLEASTSQUARES: LSQ gradient + limiter      */
+
+/* PetscLimiter types (symmetric Berger-Aftosmis-Murman form, f = 1/2 du/(grad u . dx)) */
+#define ABL_LIMITER_NONE 0
+#define ABL_LIMITER_ZERO 1
+#define ABL_LIMITER_MINMOD 2
+#define ABL_LIMITER_VANLEER 3
+#define ABL_LIMITER_VANALBADA 4
+#define ABL_LIMITER_SIN 5
+
+/* cell kinds inside one rank's local mesh */
+#define ABL_CELL_OWNED 0      /* residual written here                                          */
+#define ABL_CELL_BOUNDARY 1   /* DMPlex FV ghost cell behind a boundary face (ghost label 1)   */
+#define ABL_CELL_HALO 2       /* owned by another rank; gradient computed here, no residual    */
+#define ABL_CELL_HALO_OUTER 3 /* owned by another rank; state only (second halo layer)          */
+
+/* precision of abl_fv_rhs */
+#define ABL_PRECISION_FP64 0
+#define ABL_PRECISION_MIXED 1 /* FP32 reconstruction/flux arithmetic, FP64 e=E/rho-|u|^2/2, T solve and accumulation */
+
+/* ---- descriptors ------------------------------------------------------------------------------ */
+/* One rank's local mesh: what DMPlex + DMPlexComputeGeometryFVM hold for the FV solver.
+ * face_cells is the face support (left, right); the area-weighted normal points left -> right
+ * (PetscFVFaceGeom.normal). Cells of kind ABL_CELL_BOUNDARY have exactly one face. */
+typedef struct abl_mesh_desc {
+    int32_t dim;                  /* 1, 2 or 3 */
+    int32_t n_cells;              /* all local cells, including boundary ghost and halo cells */
+    int32_t n_faces;
+    const int32_t* face_cells;    /* [n_faces][2] */
+    const double* face_normal;    /* [n_faces][3] area-weighted normal (unused components 0) */
+    const double* face_centroid;  /* [n_faces][3] */
+    const double* cell_centroid;  /* [n_cells][3] */
+    const double* cell_volume;    /* [n_cells] */
+    const uint8_t* cell_kind;     /* [n_cells] ABL_CELL_*; NULL: every cell owned */
+    const double* face_shift;     /* [n_faces][3] periodic image shift: the right cell's centroid seen from
+                                     the left cell is cell_centroid[right] + face_shift (and the face centroid,
+                                     given in the left cell's frame, is face_centroid - face_shift in the right
+                                     cell's frame); NULL: no periodic faces */
+} abl_mesh_desc;
+
+/* Process configuration: what NavierStokesTransport / SpeciesTransport register in Setup
+ * (src/finiteVolume/processes/navierStokesTransport.cpp:35-97, speciesTransport.cpp:35-96). */
+typedef struct abl_physics_desc {
+    int32_t eos;             /* ABL_EOS_* */
+    double gamma;            /* perfect gas: specific heat ratio (default 1.4) */
+    double r_gas;            /* perfect gas: gas constant J/(kg K) (default 287) */
+    int32_t n_species;       /* densityYi components; 0 = no species field */
+    const double* nasa7;     /* [n_species][15]: T_mid, low a1..a7, high a1..a7 (cp/R = a1 + a2 T + ... ) */
+    const double* mw;        /* [n_species] molar mass kg/kmol */
+
+    int32_t flux;            /* ABL_FLUX_*; ABL_FLUX_OFF with advection = 0 disables advection */
+    double ausmpup_minf;     /* AusmpUp mInf (0 = fa = 1) */
+    double pgs_alpha;        /* pressure gradient scaling alpha (1 = none) */
+
+    int32_t reconstruction;  /* ABL_RECON_* (both conserved fields use the same PetscFV) */
+    int32_t limiter;         /* ABL_LIMITER_* */
+    double max_lim_grad;     /* CellInterpolant maxLimGrad (default 1e10) */
+
+    int32_t transport;       /* ABL_TRANSPORT_* */
+    double k, mu, diff;      /* constant model values; for CONSTANT_LEWIS: mu, prandtl in k, lewis in diff */
+
+    int32_t advection;          /* NavierStokesTransport::AdvectionFlux registered */
+    int32_t diffusion;          /* NavierStokesTransport::DiffusionFlux registered */
+    int32_t species_advection;  /* SpeciesTransport::AdvectionFlux registered */
+    int32_t species_diffusion;  /* SpeciesTransport::DiffusionSpeciesFlux + DiffusionEnergyFlux registered */
+} abl_physics_desc;
+
+typedef struct abl_fv abl_fv; /* opaque handle: one mesh + physics resident on one device */
+
+/* ---- library ---------------------------------------------------------------------------------- */
+const char* abl_last_error_string(void);
+int abl_version(void);
+int abl_device_count(int* count);
+
+/* ---- handle lifecycle ------------------------------------------------------------------------- */
+/* Upload the mesh, the geometry and the least-squares weights (built here, once, from the geometry as
+ * BuildGradientReconstruction_Internal and LeastSquaresAverage::Generate do:
+ * src/finiteVolume/cellInterpolant.cpp:641-715, src/finiteVolume/stencils/leastSquaresAverage.cpp:5-155)
+ * to device `device`. Replaces the lazy CellInterpolant/FaceInterpolant construction at
+ * src/finiteVolume/finiteVolumeSolver.cpp:241-243, 269-271. */
+int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, int device, abl_fv** out);
+int abl_fv_destroy(abl_fv* fv);
+int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells, int32_t* n_faces);
+
+/* ---- the hot path ----------------------------------------------------------------------------- */
+/* F += RHS(U) for owned cells, device pointers, on `stream` (a cudaStream_t; NULL = legacy stream).
+ * Runs the aux update (T, velocity, Y for every local cell, T guess = the resident aux T), the
+ * gradient/limiter pass and the flux passes. Replaces CellSolver::UpdateAuxFields +
+ * FiniteVolumeSolver::ComputeRHSFunction (src/solver/cellSolver.cpp:62-135,
+ * src/finiteVolume/finiteVolumeSolver.cpp:233-291). */
+int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int precision, void* stream);
+
+/* Same with host pointers (the plain PETSc Vec case): copies U in, runs abl_fv_rhs, adds into F. */
+int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision);
+
+/* Aux fields (T, u, Y) of the last evaluation / set the temperature guess used by the next one. */
+int abl_fv_get_aux(abl_fv* fv, double* aux_host);
+int abl_fv_set_aux(abl_fv* fv, const double* aux_host);
+
+/* Device status word accumulated since the last call: ABL_OK or the first ABL_ERR_* a kernel saw. */
+int abl_fv_status(abl_fv* fv);
+
+/* Number of kernel launches one abl_fv_rhs call makes at `precision` (for launch accounting). */
+int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches);
+
+/* ---- point functions (device batches; used for known-answer tests of the device physics) --------- */
+/* Flux calculator over n faces: the FluxCalculatorFunction signature
+ * (src/finiteVolume/fluxCalculator/fluxCalculator.hpp:13-14) applied element-wise on the device. */
+int abl_flux_calculator_batch(int kind, double minf, double pgs_alpha, double gamma, int64_t n, const double* uL, const double* aL,
+                              const double* rhoL, const double* pL, const double* uR, const double* aR, const double* rhoR,
+                              const double* pR, double* mass_flux, double* p12, int32_t* direction);
+
+/* ThermodynamicTemperatureFunction / ThermodynamicFunction of `property` for n conserved states
+ * conserved[n][nc] with dim = nc - 2 - n_species. If T_in is non-NULL it is the temperature argument
+ * (the *TemperatureFunction variant); otherwise T is computed first (guess 300 K, as TChem does).
+ * out[n][property size]. */
+int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved,
+                  const double* T_in, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ABLATE_FV_H */

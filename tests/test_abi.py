@@ -1,0 +1,77 @@
+"""The C-ABI library loads, exports every entry point include/ablate_fv.h declares, and rejects bad
+input on the host (no GPU needed: nothing here launches a kernel)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from ablate_b200 import _lib as L
+from ablate_b200.mesh import box_mesh
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "ablate_fv.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(abl_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(str(L.LIB_PATH))
+    names = declared_symbols()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(L.SIGNATURES), "binding table out of sync with the header"
+
+
+def test_version_and_error_string():
+    assert L.lib.abl_version() >= 1
+    assert isinstance(L.lib.abl_last_error_string(), bytes)
+
+
+def test_create_rejects_null_and_bad_descriptors():
+    h = C.c_void_p()
+    assert L.lib.abl_fv_create(None, None, 0, C.byref(h)) == L.ERR_INVALID_ARGUMENT
+    m = box_mesh((4, 4))
+    d = m.desc()
+    p = L.PhysicsDesc()
+    p.eos = 7  # unknown EOS
+    assert L.lib.abl_fv_create(C.byref(d), C.byref(p), 0, C.byref(h)) == L.ERR_INVALID_ARGUMENT
+    assert b"eos" in L.lib.abl_last_error_string()
+    p.eos = L.EOS_PERFECT_GAS
+    p.gamma, p.r_gas = 1.4, 287.0
+    p.flux = L.FLUX_RIEMANN
+    p.n_species = 4  # no compiled instance for 2D with 4 species
+    rc = L.lib.abl_fv_create(C.byref(d), C.byref(p), 0, C.byref(h))
+    assert rc == L.ERR_UNSUPPORTED
+    assert not h.value
+
+
+def test_null_handle_calls_fail_cleanly():
+    assert L.lib.abl_fv_rhs(None, 0.0, None, None, 0, None) == L.ERR_INVALID_ARGUMENT
+    assert L.lib.abl_fv_status(None) == L.ERR_INVALID_ARGUMENT
+    assert L.lib.abl_fv_destroy(None) == L.OK
+
+
+def test_batch_rejects_bad_enums_before_touching_the_device():
+    z = np.zeros(1)
+    zi = np.zeros(1, np.int32)
+    args = [L.dptr(z)] * 10
+    assert L.lib.abl_flux_calculator_batch(99, 0.0, 1.0, 1.4, 1, *args, L.iptr(zi)) == L.ERR_INVALID_ARGUMENT
+    p = L.PhysicsDesc()
+    p.eos, p.gamma, p.r_gas = L.EOS_PERFECT_GAS, 1.4, 287.0
+    assert L.lib.abl_eos_batch(C.byref(p), 4, 0, 1, L.dptr(z), None, L.dptr(z)) == L.ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.skipif(L.device_count() > 0, reason="checks the no-device path")
+def test_no_device_reported():
+    m = box_mesh((4, 4))
+    d = m.desc()
+    p = L.PhysicsDesc()
+    p.eos, p.gamma, p.r_gas, p.flux, p.advection = L.EOS_PERFECT_GAS, 1.4, 287.0, L.FLUX_AUSM, 1
+    h = C.c_void_p()
+    assert L.lib.abl_fv_create(C.byref(d), C.byref(p), 0, C.byref(h)) == L.ERR_NO_DEVICE
