@@ -35,6 +35,7 @@ RECON_UPWIND, RECON_LEASTSQUARES = 0, 1
 LIMITER_NONE, LIMITER_ZERO, LIMITER_MINMOD, LIMITER_VANLEER, LIMITER_VANALBADA, LIMITER_SIN = range(6)
 CELL_OWNED, CELL_BOUNDARY, CELL_HALO, CELL_HALO_OUTER = range(4)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+RHS_OVERWRITE = 0x100
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -70,10 +71,14 @@ SIGNATURES = {
     "abl_fv_sizes": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "abl_fv_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
+    "abl_fv_update_aux": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_update_aux_host": (C.c_int, [C.c_void_p, _dp]),
     "abl_fv_get_aux": (C.c_int, [C.c_void_p, _dp]),
     "abl_fv_set_aux": (C.c_int, [C.c_void_p, _dp]),
     "abl_fv_status": (C.c_int, [C.c_void_p]),
     "abl_fv_launch_count": (C.c_int, [C.c_void_p, C.c_int, _ip]),
+    "abl_fv_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "abl_fv_profile_read": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_float), C.c_char_p]),
     "abl_flux_calculator_batch": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64] + [_dp] * 10 + [_ip]),
     "abl_eos_batch": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, _dp, _dp, _dp]),
 }

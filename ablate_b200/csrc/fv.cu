@@ -73,11 +73,22 @@ struct abl_fv {
     // resident mesh + geometry
     DevBuf<int2> face_cells;
     DevBuf<uint8_t> kind, cone_side, face_boundary;
-    DevBuf<int> cone_ptr, cone_face, cone_nbr, flux_faces;
-    DevBuf<double> normal, fdx, vol, cgrad, fgrad;
+    DevBuf<int> cone_ptr, cone_face, cone_nbr;
+    DevBuf<double> fdx, ivol, cgrad, fgrad;
     DevBuf<double> nasa7, mw, inv_mw, href;
+    // tiles
+    DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
+    DevBuf<int2> tf_cells;
+    DevBuf<double> tf_normal, tf_fdx;
+    DevBuf<uint16_t> tc_face;
+    int tile_smem = 0;
+    // optional per-kernel timing of the last abl_fv_rhs call
+    bool profile = false;
+    int n_marks = 0;
+    cudaEvent_t marks[8] = {};
+    const char* mark_names[8] = {};
     // work buffers
-    DevBuf<double> aux, fflux;
+    DevBuf<double> aux;
     DevBuf<double> grad64, agrad64;
     DevBuf<float> grad32, agrad32;
     DevBuf<int> status;
@@ -87,6 +98,15 @@ struct abl_fv {
 };
 
 namespace {
+
+// record a timing mark (event) before the next launch when profiling is on
+void mark(abl_fv* fv, const char* name, cudaStream_t s) {
+    if (!fv->profile || fv->n_marks >= 8) return;
+    if (!fv->marks[fv->n_marks]) ABL_CUDA(cudaEventCreate(&fv->marks[fv->n_marks]));
+    ABL_CUDA(cudaEventRecord(fv->marks[fv->n_marks], s));
+    fv->mark_names[fv->n_marks] = name;
+    fv->n_marks++;
+}
 
 int fail(const AblError& e) {
     g_last_error = e.what();
@@ -184,54 +204,73 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
 }
 
 // ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
+template <int DIM, int NS, class G>
+void launch_tile(abl_fv* fv, const double* U, const G* grad, const G* agrad, double* F, int overwrite, cudaStream_t s) {
+    auto kern = k_tile_flux<DIM, NS, G>;
+    static thread_local int configured = -1;
+    if (configured != fv->tile_smem) {
+        ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, fv->tile_smem));
+        configured = fv->tile_smem;
+    }
+    kern<<<fv->mesh.n_tiles, 128, fv->tile_smem, s>>>(fv->mesh, fv->phys, U, fv->aux.p, grad, agrad, F, overwrite, fv->status.p);
+    check_launch();
+}
+
 template <int DIM, int NS>
-void run_rhs(abl_fv* fv, const double* U, double* F, int precision, cudaStream_t s) {
+void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
     const DevMesh& M = fv->mesh;
     const Phys& P = fv->phys;
+    fv->n_marks = 0;
     if (fv->need_aux) {
+        mark(fv, "k_aux", s);
         k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, P, U, fv->aux.p, fv->status.p);
         check_launch();
     }
+    const bool grads = fv->need_state_grad || fv->need_aux_grad;
     if (precision == ABL_PRECISION_MIXED) {
-        if (fv->need_state_grad || fv->need_aux_grad) {
+        if (grads) {
+            mark(fv, "k_gradient", s);
             k_gradient<DIM, NS, float><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad32.p, fv->agrad32.p,
                                                                                    fv->need_state_grad, fv->need_aux_grad);
             check_launch();
         }
-        if (M.n_flux_faces > 0) {
-            k_face_flux<DIM, NS, float><<<blocks_for(M.n_flux_faces, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad32.p, fv->agrad32.p,
-                                                                                          fv->fflux.p, fv->status.p);
-            check_launch();
-        }
+        mark(fv, "k_tile_flux", s);
+        if (M.n_tiles > 0) launch_tile<DIM, NS, float>(fv, U, fv->grad32.p, fv->agrad32.p, F, overwrite, s);
     } else {
-        if (fv->need_state_grad || fv->need_aux_grad) {
+        if (grads) {
+            mark(fv, "k_gradient", s);
             k_gradient<DIM, NS, double><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p,
                                                                                     fv->need_state_grad, fv->need_aux_grad);
             check_launch();
         }
-        if (M.n_flux_faces > 0) {
-            k_face_flux<DIM, NS, double><<<blocks_for(M.n_flux_faces, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p,
-                                                                                           fv->fflux.p, fv->status.p);
-            check_launch();
-        }
+        mark(fv, "k_tile_flux", s);
+        if (M.n_tiles > 0) launch_tile<DIM, NS, double>(fv, U, fv->grad64.p, fv->agrad64.p, F, overwrite, s);
     }
-    k_gather<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, fv->fflux.p, F, fv->status.p);
+    mark(fv, "end", s);
+}
+
+template <int DIM, int NS>
+void run_aux(abl_fv* fv, const double* U, cudaStream_t s) {
+    k_aux<DIM, NS><<<blocks_for(fv->mesh.n_cells, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->aux.p, fv->status.p);
     check_launch();
 }
 
-void dispatch_rhs(abl_fv* fv, const double* U, double* F, int precision, cudaStream_t s) {
-    const int key = fv->dim * 100 + fv->ns;
-    switch (key) {
-        case 100: return run_rhs<1, 0>(fv, U, F, precision, s);
-        case 200: return run_rhs<2, 0>(fv, U, F, precision, s);
-        case 202: return run_rhs<2, 2>(fv, U, F, precision, s);
-        case 300: return run_rhs<3, 0>(fv, U, F, precision, s);
-        case 302: return run_rhs<3, 2>(fv, U, F, precision, s);
-        case 305: return run_rhs<3, 5>(fv, U, F, precision, s);
-        case 309: return run_rhs<3, 9>(fv, U, F, precision, s);
-    }
-    throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for dim " + std::to_string(fv->dim) + " with " + std::to_string(fv->ns) +
-                                            " species (compiled: dim 1/2/3 without species, dim 2 with 2, dim 3 with 2, 5 or 9)");
+#define ABL_DISPATCH(fv, FN, ...)                                                                                                  \
+    do {                                                                                                                           \
+        switch ((fv)->dim * 100 + (fv)->ns) {                                                                                      \
+            case 100: FN<1, 0>(fv, __VA_ARGS__); break;                                                                            \
+            case 200: FN<2, 0>(fv, __VA_ARGS__); break;                                                                            \
+            case 202: FN<2, 2>(fv, __VA_ARGS__); break;                                                                            \
+            case 300: FN<3, 0>(fv, __VA_ARGS__); break;                                                                            \
+            case 302: FN<3, 2>(fv, __VA_ARGS__); break;                                                                            \
+            case 305: FN<3, 5>(fv, __VA_ARGS__); break;                                                                            \
+            case 309: FN<3, 9>(fv, __VA_ARGS__); break;                                                                            \
+            default: throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for this dimension/species count");          \
+        }                                                                                                                          \
+    } while (0)
+
+void dispatch_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
+    ABL_DISPATCH(fv, run_rhs, U, F, precision, overwrite, s);
 }
 
 bool rhs_supported(int dim, int ns) {
@@ -402,7 +441,8 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->n_flux_faces = (int)h.flux_faces.size();
         fv->need_state_grad = lsq;
         fv->need_aux_grad = dif;
-        fv->need_aux = true;
+        // the mixture EOS keeps T resident (secant guess + face temperatures); a perfect gas recomputes it
+        fv->need_aux = physics->eos == ABL_EOS_NASA7;
         upload_species(physics, fv->phys, fv->nasa7, fv->mw, fv->inv_mw, fv->href);
 
         fv->face_cells.upload(reinterpret_cast<const int2*>(h.face_cells.data()), h.n_faces);
@@ -412,10 +452,29 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->cone_nbr.upload(h.cone_nbr.data(), h.cone_nbr.size());
         fv->cone_side.upload(h.cone_side.data(), h.cone_side.size());
         fv->face_boundary.upload(h.face_boundary.data(), h.face_boundary.size());
-        fv->flux_faces.upload(h.flux_faces.data(), h.flux_faces.size());
-        fv->normal.upload(mesh->face_normal, 3 * (size_t)h.n_faces);
         fv->fdx.upload(h.fdx.data(), h.fdx.size());
-        fv->vol.upload(mesh->cell_volume, h.n_cells);
+        {
+            std::vector<double> iv(h.n_cells);
+            for (int c = 0; c < h.n_cells; c++) iv[c] = 1.0 / mesh->cell_volume[c];
+            fv->ivol.upload(iv.data(), iv.size());
+        }
+        // cell tiles for the fused flux kernel: the largest tile whose face fluxes fit in shared memory
+        const int nc_ = 2 + h.dim + physics->n_species;
+        int tile = 256;
+        Tiles tl = build_tiles(h, mesh, tile);
+        while ((size_t)tl.max_faces * nc_ * sizeof(double) > 200 * 1024 && tile > 16) {
+            tile /= 2;
+            tl = build_tiles(h, mesh, tile);
+        }
+        fv->tile_smem = (int)((size_t)std::max(tl.max_faces, 1) * nc_ * sizeof(double));
+        fv->tile_cell_ptr.upload(tl.cell_ptr.data(), tl.cell_ptr.size());
+        fv->tile_cells.upload(tl.cells.data(), tl.cells.size());
+        fv->tile_face_ptr.upload(tl.face_ptr.data(), tl.face_ptr.size());
+        fv->tf_cells.upload(reinterpret_cast<const int2*>(tl.tf_cells.data()), tl.tf_cells.size() / 2);
+        fv->tf_normal.upload(tl.tf_normal.data(), tl.tf_normal.size());
+        fv->tf_fdx.upload(tl.tf_fdx.data(), tl.tf_fdx.size());
+        fv->tc_fptr.upload(tl.tc_fptr.data(), tl.tc_fptr.size());
+        fv->tc_face.upload(tl.tc_face.data(), tl.tc_face.size());
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
 
@@ -425,7 +484,6 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             for (int c = 0; c < fv->n_cells; c++) a0[(size_t)c * fv->naux] = 300.0;  // temperature guess (TChem::TemperatureFunction uses 300 K)
             ABL_CUDA(cudaMemcpy(fv->aux.p, a0.data(), a0.size() * sizeof(double), cudaMemcpyHostToDevice));
         }
-        fv->fflux.alloc((size_t)fv->n_faces * fv->nc);
         if (lsq) {
             fv->grad64.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
             fv->grad32.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
@@ -449,12 +507,19 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.cone_nbr = fv->cone_nbr.p;
         M.cone_side = fv->cone_side.p;
         M.face_boundary = fv->face_boundary.p;
-        M.flux_faces = fv->flux_faces.p;
-        M.normal = fv->normal.p;
         M.fdx = fv->fdx.p;
-        M.vol = fv->vol.p;
+        M.ivol = fv->ivol.p;
         M.cgrad = fv->cgrad.p;
         M.fgrad = fv->fgrad.p;
+        M.n_tiles = tl.n_tiles;
+        M.tile_cell_ptr = fv->tile_cell_ptr.p;
+        M.tile_cells = fv->tile_cells.p;
+        M.tile_face_ptr = fv->tile_face_ptr.p;
+        M.tf_cells = fv->tf_cells.p;
+        M.tf_normal = fv->tf_normal.p;
+        M.tf_fdx = fv->tf_fdx.p;
+        M.tc_fptr = fv->tc_fptr.p;
+        M.tc_face = fv->tc_face.p;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();
     });
@@ -463,8 +528,32 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
 int abl_fv_destroy(abl_fv* fv) {
     if (!fv) return ABL_OK;
     cudaSetDevice(fv->device);
+    for (auto& e : fv->marks)
+        if (e) cudaEventDestroy(e);
     delete fv;
     return ABL_OK;
+}
+
+int abl_fv_profile(abl_fv* fv, int enable) {
+    if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
+    fv->profile = enable != 0;
+    fv->n_marks = 0;
+    return ABL_OK;
+}
+
+int abl_fv_profile_read(abl_fv* fv, int32_t* n, float* ms, char* names) {
+    return guarded([&] {
+        if (!fv || !n || !ms || !names) throw std::invalid_argument("NULL argument");
+        *n = 0;
+        if (fv->n_marks < 2) return;
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_CUDA(cudaEventSynchronize(fv->marks[fv->n_marks - 1]));
+        for (int i = 0; i + 1 < fv->n_marks; i++) {
+            ABL_CUDA(cudaEventElapsedTime(&ms[i], fv->marks[i], fv->marks[i + 1]));
+            std::snprintf(names + 32 * i, 32, "%s", fv->mark_names[i]);
+        }
+        *n = fv->n_marks - 1;
+    });
 }
 
 int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells, int32_t* n_faces) {
@@ -480,9 +569,32 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
     (void)time;
     return guarded([&] {
         if (!fv || !U_dev || !F_dev) throw std::invalid_argument("abl_fv_rhs: NULL argument");
+        const int overwrite = (precision & ABL_RHS_OVERWRITE) != 0;
+        precision &= ~ABL_RHS_OVERWRITE;
         if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
         ABL_CUDA(cudaSetDevice(fv->device));
-        dispatch_rhs(fv, U_dev, F_dev, precision, static_cast<cudaStream_t>(stream));
+        dispatch_rhs(fv, U_dev, F_dev, precision, overwrite, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_update_aux(abl_fv* fv, const double* U_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev) throw std::invalid_argument("abl_fv_update_aux: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_DISPATCH(fv, run_aux, U_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_update_aux_host(abl_fv* fv, const double* U_host) {
+    return guarded([&] {
+        if (!fv || !U_host) throw std::invalid_argument("abl_fv_update_aux_host: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->hU.n != n) fv->hU.alloc(n);
+        ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        int rc = abl_fv_update_aux(fv, fv->hU.p, nullptr);
+        if (rc != ABL_OK) throw AblError(rc, g_last_error);
+        ABL_CUDA(cudaDeviceSynchronize());
     });
 }
 
@@ -495,7 +607,7 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
         if (fv->hF.n != n) fv->hF.alloc(n);
         ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
         ABL_CUDA(cudaMemcpy(fv->hF.p, F_host, n * sizeof(double), cudaMemcpyHostToDevice));
-        int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision, nullptr);
+        int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision & ~ABL_RHS_OVERWRITE, nullptr);
         if (rc != ABL_OK) throw AblError(rc, g_last_error);
         ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
     });
@@ -534,10 +646,10 @@ int abl_fv_status(abl_fv* fv) {
 int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches) {
     if (!fv || !launches) return fail(ABL_ERR_INVALID_ARGUMENT, "NULL argument");
     (void)precision;
-    int n = 1;  // gather
+    int n = 0;
     if (fv->need_aux) n++;
     if (fv->need_state_grad || fv->need_aux_grad) n++;
-    if (fv->n_flux_faces > 0) n++;
+    if (fv->mesh.n_tiles > 0) n++;
     *launches = n;
     return ABL_OK;
 }

@@ -30,6 +30,23 @@ ABL_HD R pmax(R a, R b) { return a < b ? b : a; }
 template <class R>
 ABL_HD R sqr(R a) { return a * a; }
 
+// FP64 reciprocal from an FP32 seed and two Newton steps (relative error below one ulp of the result
+// for |x| in the FP32 normal range); zero, subnormal-in-FP32, infinite, NaN and out-of-range inputs
+// take the IEEE division so their special values are exactly those of 1/x.
+ABL_HD double rcp64(double x) {
+#ifdef __CUDA_ARCH__
+    const float xf = __double2float_rn(x);
+    const float ax = fabsf(xf);
+    if (!(ax > 1.2e-38f && ax < 3.0e38f)) return 1.0 / x;
+    double r = (double)__frcp_rn(xf);
+    r = r * fma(-x, r, 2.0);
+    r = r * fma(-x, r, 2.0);
+    return r;
+#else
+    return 1.0 / x;
+#endif
+}
+ABL_HD float rcp64(float x) { return 1.0f / x; }
 ABL_HD double dsqrt(double x) { return sqrt(x); }
 ABL_HD float dsqrt(float x) { return sqrtf(x); }
 ABL_HD double dabs(double x) { return fabs(x); }
@@ -58,7 +75,7 @@ constexpr double kTref = 298.15;             // TChemBase::TREF (src/eos/tChemBa
 template <class R>
 ABL_HD int flux_ausm(R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R pR, R* mf, R* p12) {
     const R one = R(1), half = R(0.5), quarter = R(0.25), two = R(2);
-    R Mm = uR / aR, sMm, sPm;
+    R Mm = uR * rcp64(aR), sMm, sPm;
     if (dabs(Mm) <= one) {
         sMm = -quarter * sqr(Mm - one);
         sPm = -(sMm) * (two + Mm);
@@ -66,7 +83,7 @@ ABL_HD int flux_ausm(R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R pR, R* mf, 
         sMm = half * (Mm - dabs(Mm));
         sPm = (sMm) / Mm;
     }
-    R Mp = uL / aL, sMp, sPp;
+    R Mp = uL * rcp64(aL), sMp, sPp;
     if (dabs(Mp) <= one) {
         sMp = quarter * sqr(Mp + one);
         sPp = (sMp) * (two - Mp);
@@ -118,10 +135,11 @@ ABL_HD int flux_ausmpup(R mInf, R pgsAlpha, R uL, R aL, R rhoL, R pL, R uR, R aR
     using A = Ausmpup<R>;
     const R Kp = R(0.25), Ku = R(0.75), sigma = R(0.25);
     R rho12 = R(0.5) * (rhoL + rhoR);
-    R a12 = R(0.5) * (aL + aR) / pgsAlpha;
-    R mL = uL / a12;
-    R mR = uR / a12;
-    R mBar2 = (sqr(uL) + sqr(uR)) / (R(2) * a12 * a12);
+    R a12 = R(0.5) * (aL + aR) * rcp64(pgsAlpha);
+    const R ia12 = rcp64(a12);
+    R mL = uL * ia12;
+    R mR = uR * ia12;
+    R mBar2 = (sqr(uL) + sqr(uR)) * (R(0.5) * ia12 * ia12);
     R fa = R(1);
     if (mInf > R(0)) {
         R mInf2 = sqr(mInf);
@@ -129,7 +147,7 @@ ABL_HD int flux_ausmpup(R mInf, R pgsAlpha, R uL, R aL, R rhoL, R pL, R uR, R aR
         R mO = dsqrt(mO2);
         fa = mO * (R(2) - mO);
     }
-    R m12 = A::M4P(mL) + A::M4M(mR) - (Kp / fa) * pmax(R(1) - (sigma * mBar2), R(0)) * (pR - pL) / (rho12 * a12 * a12 * pgsAlpha * pgsAlpha);
+    R m12 = A::M4P(mL) + A::M4M(mR) - (Kp * rcp64(fa)) * pmax(R(1) - (sigma * mBar2), R(0)) * (pR - pL) * rcp64(rho12 * a12 * a12 * pgsAlpha * pgsAlpha);
     int dir;
     if (m12 > R(0)) {
         dir = ABL_DIR_LEFT;
@@ -142,7 +160,7 @@ ABL_HD int flux_ausmpup(R mInf, R pgsAlpha, R uL, R aL, R rhoL, R pL, R uR, R aR
         R p5Plus = A::P5P(mL, fa);
         R p5Minus = A::P5M(mR, fa);
         R v = p5Plus * pL + p5Minus * pR - Ku * p5Plus * p5Minus * rho12 * fa * a12 * a12 * pgsAlpha * pgsAlpha * (mR - mL);
-        *p12 = v / sqr(pgsAlpha);
+        *p12 = v * rcp64(sqr(pgsAlpha));
     }
     return dir;
 }
@@ -284,6 +302,125 @@ ABL_HD int flux_calc(const Phys& P, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR
 }
 
 // ------------------------------------------------------------------------------------------------
+// Split form of the AUSM-family fluxes for the mixed-precision path.
+//
+// The face mass flux and pressure are each written exactly (in exact arithmetic) as a large central
+// part plus a small dissipative part:
+//   mass flux  m A = 1/2 rho_up (u_L + u_R).n        +  [upwinding and Mach-splitting terms] A
+//   pressure   p12 = (p_L + p_R) / 2 / alpha^2       +  [P5/P terms times (p_L - p_R), (M_R - M_L)] / alpha^2
+// The central parts are evaluated in FP64 (a handful of multiplies, no division or square root); the
+// dissipative parts, which carry all of the sound speeds, Mach numbers, polynomial splittings and
+// branches, in FP32. Every difference of nearly equal quantities (M_L - M_R, p_L - p_R, u_L - u_R) is
+// formed from FP64 inputs before rounding to FP32, and the differences of splitting polynomials are
+// evaluated as (M_L - M_R) times their divided difference, so the FP32 rounding error is relative to
+// the small terms, not to the fluxes. The identities used are exact for the reference formulas:
+//   AUSM  : M+(M) = M/2 + g(M), M-(M) = M/2 - g(M), g = M^2/4 + 1/4 (|M| <= 1), |M|/2 otherwise;
+//           P+(M) + P-(M) = 1; P-(M) = (M^3 - 3M + 2)/4 on |M| <= 1
+//   AUSM+ : M4+(m) = m/2 + g4(m), M4-(m) = m/2 - g4(m), g4 = m^4/8 + 3/8 (|m| < 1, beta = 1/8), |m|/2 otherwise;
+//           P5+(m) + P5-(m) = 1; P5-(m) = 1/2 - (3/4 + a) m + (1/4 + 2a) m^3 - a m^5 on |m| < 1
+struct SplitFlux {
+    double mA_c;  // central mass flux times area (FP64)
+    float mA_d;   // dissipative mass flux times area
+    double p_c;   // central interface pressure (FP64)
+    float p_d;    // dissipative interface pressure
+    int dir;
+};
+
+// rho, p: face states (FP64); unA = u.n (velocity dotted with the area-weighted normal, FP64);
+// a: sound speeds (FP32); area = |n| (FP32)
+template <int KIND>
+ABL_HD SplitFlux flux_split(const Phys& P, double rhoL, double pL, double unAL, float aL, double rhoR, double pR, double unAR, float aR,
+                            float area) {
+    SplitFlux r;
+    const float iA = 1.0f / area;
+    const float uL = float(unAL) * iA, uR = float(unAR) * iA;
+    const float du = float(unAL - unAR) * iA;      // u_L - u_R, from the FP64 difference
+    const float dp = float(0.5 * (pL - pR));       // (p_L - p_R) / 2
+    const double pbar = 0.5 * (pL + pR);
+    if constexpr (KIND == ABL_FLUX_AUSM) {
+        // Ausm::AusmFunction (ausm.cpp:2-43) in split form
+        const float ML = uL / aL, MR = uR / aR;
+        const bool subL = fabsf(ML) <= 1.f, subR = fabsf(MR) <= 1.f;
+        // g(ML) - g(MR)
+        float dg;
+        const float dM = du / aL + uR * (aR - aL) / (aL * aR);  // ML - MR
+        if (subL && subR)
+            dg = 0.25f * dM * (ML + MR);
+        else
+            dg = (subL ? 0.25f * ML * ML + 0.25f : 0.5f * fabsf(ML)) - (subR ? 0.25f * MR * MR + 0.25f : 0.5f * fabsf(MR));
+        const float sMp = subL ? 0.25f * (ML + 1.f) * (ML + 1.f) : 0.5f * (ML + fabsf(ML));
+        const float sMm = subR ? -0.25f * (MR - 1.f) * (MR - 1.f) : 0.5f * (MR - fabsf(MR));
+        const float m = sMm + sMp;
+        const bool left = !(m < 0.f);
+        r.dir = left ? ABL_DIR_LEFT : ABL_DIR_RIGHT;
+        const double rho_up = left ? rhoL : rhoR;
+        const float a_up = left ? aL : aR;
+        // m a_up = (uL + uR)/2 + [uR (aL - aR)/aR or uL (aR - aL)/aL]/2 + a_up (g(ML) - g(MR))
+        const float skew = left ? 0.5f * uR * (aL - aR) / aR : 0.5f * uL * (aR - aL) / aL;
+        r.mA_c = 0.5 * rho_up * (unAL + unAR);
+        r.mA_d = float(rho_up) * (skew + a_up * dg) * area;
+        // p12 = pbar (P+(ML) + P-(MR)) + dp (P+(ML) - P-(MR)), P+(ML) + P-(MR) = 1 + P-(MR) - P-(ML)
+        const float sPp = subL ? sMp * (2.f - ML) : sMp / ML;
+        const float sPm = subR ? -sMm * (2.f + MR) : sMm / MR;
+        float dP;  // P-(MR) - P-(ML)
+        if (subL && subR)
+            dP = -dM * 0.25f * (ML * ML + ML * MR + MR * MR - 3.f);
+        else
+            dP = sPm - (subL ? 0.25f * (ML - 1.f) * (ML - 1.f) * (2.f + ML) : (0.5f * (ML - fabsf(ML))) / ML);
+        r.p_c = pbar;
+        r.p_d = float(pbar) * dP + dp * (sPp - sPm);
+        return r;
+    } else {
+        // AusmpUp::AusmpUpFunction (ausmpUp.cpp:5-53) in split form
+        const float alpha = float(P.alpha), mInf = float(P.minf);
+        const float Kp = 0.25f, Ku = 0.75f, sigma = 0.25f;
+        const float rho12 = float(0.5 * (rhoL + rhoR));
+        const float a12 = 0.5f * (aL + aR) / alpha;
+        const float mL = uL / a12, mR = uR / a12;
+        const float dm = du / a12;  // mL - mR
+        const float mBar2 = (uL * uL + uR * uR) / (2.f * a12 * a12);
+        float fa = 1.f;
+        if (mInf > 0.f) {
+            const float mO2 = pmin(1.f, pmax(mBar2, mInf * mInf));
+            const float mO = sqrtf(mO2);
+            fa = mO * (2.f - mO);
+        }
+        const bool subL = fabsf(mL) < 1.f, subR = fabsf(mR) < 1.f;
+        float dg;  // g4(mL) - g4(mR)
+        if (subL && subR)
+            dg = 0.125f * dm * (mL + mR) * (mL * mL + mR * mR);
+        else
+            dg = (subL ? 0.125f * mL * mL * mL * mL + 0.375f : 0.5f * fabsf(mL)) - (subR ? 0.125f * mR * mR * mR * mR + 0.375f : 0.5f * fabsf(mR));
+        const float Mp = (Kp / fa) * pmax(1.f - sigma * mBar2, 0.f) * (-2.f * dp) / (rho12 * a12 * a12 * alpha * alpha);
+        // m12 = (mL + mR)/2 + dg - Mp; the sign decides the upwind side
+        const float m12 = 0.5f * (mL + mR) + dg - Mp;
+        const bool left = m12 > 0.f;
+        r.dir = left ? ABL_DIR_LEFT : ABL_DIR_RIGHT;
+        const double rho_up = left ? rhoL : rhoR;
+        // m a12 rho = rho (uL + uR)/2 + rho a12 (dg - Mp)
+        r.mA_c = 0.5 * rho_up * (unAL + unAR);
+        r.mA_d = float(rho_up) * a12 * (dg - Mp) * area;
+        // P5 splittings
+        using A = Ausmpup<float>;
+        const float p5p = A::P5P(mL, fa), p5m = A::P5M(mR, fa);
+        float dP;  // P5-(mR) - P5-(mL)
+        if (subL && subR) {
+            const float a5 = 3.f / 16.f * (-4.f + 5.f * fa * fa);
+            const float s3 = mL * mL + mL * mR + mR * mR;
+            const float s5 = mL * mL * mL * mL + mL * mL * mL * mR + mL * mL * mR * mR + mL * mR * mR * mR + mR * mR * mR * mR;
+            dP = -dm * (-(0.75f + a5) + (0.25f + 2.f * a5) * s3 - a5 * s5);
+        } else {
+            dP = p5m - A::P5M(mL, fa);
+        }
+        const float ia2 = 1.f / (alpha * alpha);
+        const float pu = -Ku * p5p * p5m * rho12 * fa * a12 * a12 * alpha * alpha * (-dm);  // (mR - mL) = -dm
+        r.p_c = pbar / (double(P.alpha) * double(P.alpha));
+        r.p_d = (float(pbar) * dP + dp * (p5p - p5m) + pu) * ia2;
+        return r;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // NASA-7 mixture thermodynamics (always FP64: the secant temperature solve and the energies it
 // differences need the full mantissa)
 // ------------------------------------------------------------------------------------------------
@@ -301,9 +438,10 @@ ABL_HD double nasa_cp_molar(const double* c, double T) {
 // src/eos/tChem.cpp:581-602); ns may be a compile-time constant after inlining.
 ABL_HD void fill_y(int ns, double rho, const double* rhoY, double* ys) {
     double sum = 0.0;
+    const double irho = rcp64(rho);
 #pragma unroll
     for (int s = 0; s < ns - 1; s++) {
-        double y = pmax(0.0, rhoY[s] / rho);
+        double y = pmax(0.0, rhoY[s] * irho);
         y = pmin(1.0, y);
         ys[s] = y;
         sum += y;
@@ -384,11 +522,11 @@ struct Decoded {
 // Internal energy recovery e = E/rho - |u|^2/2 (always FP64).
 template <int DIM>
 ABL_HD double internal_energy(const double* U) {
-    const double rho = U[0];
+    const double irho = rcp64(U[0]);
     double ke = 0.0;
 #pragma unroll
-    for (int i = 0; i < DIM; i++) ke += sqr(U[2 + i] / rho);
-    return U[1] / rho - 0.5 * ke;
+    for (int i = 0; i < DIM; i++) ke += sqr(U[2 + i] * irho);
+    return U[1] * irho - 0.5 * ke;
 }
 
 // Decode with the *TemperatureFunction variants at T(U, guess):
@@ -400,30 +538,27 @@ ABL_HD Decoded decode(const Phys& P, int ns, const double* U, double Tguess, boo
     Decoded d;
     const double rho = U[0];
     if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) {
+        // T = e/cv, e(T) = cv T, p(T) = R rho T, a(T) = sqrt(gamma p / rho) = sqrt(gamma R T)
         const double e = internal_energy<DIM>(U);
         const double cv = P.r_gas / (P.gamma - 1.0);
-        d.T = e / cv;
+        d.T = e * rcp64(cv);
         d.e = d.T * cv;
-        const double pr = P.r_gas * rho * d.T;
-        d.a = sqrt(P.gamma * (pr) / rho);
-        d.p = pr;
+        d.p = P.r_gas * rho * d.T;
+        d.a = sqrt(P.gamma * P.r_gas * d.T);
         return d;
     }
     double ys[NSMAX > 0 ? NSMAX : 1];
     fill_y(ns, rho, U + 2 + DIM, ys);
-    double speedSquare = 0.0;
-#pragma unroll
-    for (int i = 0; i < DIM; i++) speedSquare += sqr(U[2 + i] / rho);
-    const double eRef = U[1] / rho - 0.5 * speedSquare;
+    const double eRef = internal_energy<DIM>(U);
     d.T = nasa_temperature(P, ns, ys, eRef, Tguess, ok);
     d.e = e_sens(P, ns, ys, d.T);
     const double cp = mixture_cp(P, ns, ys, d.T);
     const double mwMix = mixture_mw(P, ns, ys);
     const double R = kRuniv / mwMix;
     const double cv = cp - R;
-    const double gamma = cp / cv;
+    const double gamma = cp * rcp64(cv);
     d.a = sqrt(gamma * R * d.T);
-    d.p = rho * kRuniv * d.T / mwMix;
+    d.p = rho * R * d.T;
     return d;
 }
 
@@ -432,14 +567,11 @@ template <int DIM, int NSMAX>
 ABL_HD double temperature(const Phys& P, int ns, const double* U, double Tguess, bool* ok) {
     if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) {
         const double e = internal_energy<DIM>(U);
-        return e / (P.r_gas / (P.gamma - 1.0));
+        return e * rcp64(P.r_gas / (P.gamma - 1.0));
     }
     double ys[NSMAX > 0 ? NSMAX : 1];
     fill_y(ns, U[0], U + 2 + DIM, ys);
-    double speedSquare = 0.0;
-#pragma unroll
-    for (int i = 0; i < DIM; i++) speedSquare += sqr(U[2 + i] / U[0]);
-    const double eRef = U[1] / U[0] - 0.5 * speedSquare;
+    const double eRef = internal_energy<DIM>(U);
     return nasa_temperature(P, ns, ys, eRef, Tguess, ok);
 }
 

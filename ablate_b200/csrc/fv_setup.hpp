@@ -9,6 +9,7 @@
 // The pseudo-inverse is computed by Householder QR of the offset matrix (full column rank) or by the
 // minimum-norm formula B^T (B B^T)^-1 (fewer offsets than dimensions: a boundary ghost cell).
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
@@ -103,6 +104,101 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
                 W[i * dim + d] = s;
             }
     }
+}
+
+// Cell tiles for the fused flux kernel: owned cells sorted along a Morton curve of their centroids
+// and cut into runs of at most `tile_cells` cells (on power-of-two boxes each run is a compact block).
+// Every tile lists all flux faces of its cells (faces shared by two tiles appear in both lists) in
+// ascending global face order, with the face geometry copied into tile order so the kernel streams
+// it, and for every tile cell the (local face, side) pairs in ascending face order.
+struct Tiles {
+    int n_tiles = 0;
+    int max_faces = 0;                    // largest per-tile face count (sizes shared memory)
+    std::vector<int32_t> cell_ptr;        // [n_tiles+1] into cells
+    std::vector<int32_t> cells;           // owned cells grouped by tile
+    std::vector<int32_t> face_ptr;        // [n_tiles+1] into the tile-face records
+    std::vector<int32_t> tf_cells;        // [ntf][2] global left/right cell
+    std::vector<double> tf_normal;        // [ntf][3]
+    std::vector<double> tf_fdx;           // [ntf][6] face centroid minus each side's centroid
+    std::vector<int32_t> tc_fptr;         // [n_owned+1] per tile cell into tc_face
+    std::vector<uint16_t> tc_face;        // local face index | side << 15
+};
+
+inline uint64_t morton_spread(uint64_t x, int dim) {
+    if (dim == 1) return x;
+    uint64_t r = 0;
+    for (int b = 0; b < (dim == 2 ? 31 : 21); b++) r |= ((x >> b) & 1ull) << (b * dim);
+    return r;
+}
+
+inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cells) {
+    Tiles t;
+    const int dim = h.dim;
+    std::vector<int32_t> owned;
+    for (int c = 0; c < h.n_cells; c++)
+        if (h.kind[c] == ABL_CELL_OWNED) owned.push_back(c);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int c : owned)
+        for (int d = 0; d < dim; d++) {
+            lo[d] = std::min(lo[d], m->cell_centroid[3 * (size_t)c + d]);
+            hi[d] = std::max(hi[d], m->cell_centroid[3 * (size_t)c + d]);
+        }
+    const int bits = dim == 1 ? 62 : (dim == 2 ? 31 : 21);
+    const double scale = std::ldexp(1.0, bits) - 1.0;
+    std::vector<std::pair<uint64_t, int32_t>> keyed(owned.size());
+    for (size_t i = 0; i < owned.size(); i++) {
+        const int c = owned[i];
+        uint64_t key = 0;
+        for (int d = 0; d < dim; d++) {
+            const double span = hi[d] - lo[d];
+            const double u = span > 0 ? (m->cell_centroid[3 * (size_t)c + d] - lo[d]) / span : 0.0;
+            key |= morton_spread((uint64_t)(u * scale), dim) << d;
+        }
+        keyed[i] = {key, c};
+    }
+    std::sort(keyed.begin(), keyed.end());
+    const int n = (int)keyed.size();
+    t.n_tiles = (n + tile_cells - 1) / tile_cells;
+    t.cell_ptr.resize(t.n_tiles + 1);
+    t.cells.resize(n);
+    for (int i = 0; i < n; i++) t.cells[i] = keyed[i].second;
+    for (int k = 0; k <= t.n_tiles; k++) t.cell_ptr[k] = std::min(n, k * tile_cells);
+    std::vector<int32_t> local(h.n_cells, -1);
+    std::vector<int32_t> faces;
+    t.face_ptr.push_back(0);
+    t.tc_fptr.assign(n + 1, 0);
+    std::vector<std::vector<uint16_t>> lists;
+    for (int k = 0; k < t.n_tiles; k++) {
+        const int cb = t.cell_ptr[k], ce = t.cell_ptr[k + 1];
+        faces.clear();
+        for (int j = cb; j < ce; j++) {
+            const int c = t.cells[j];
+            local[c] = j - cb;
+            for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) faces.push_back(h.cone_face[i]);
+        }
+        std::sort(faces.begin(), faces.end());
+        faces.erase(std::unique(faces.begin(), faces.end()), faces.end());
+        if (faces.size() > 0x7fff) throw std::invalid_argument("tile has too many faces");
+        t.max_faces = std::max(t.max_faces, (int)faces.size());
+        lists.assign(ce - cb, {});
+        for (size_t i = 0; i < faces.size(); i++) {
+            const int f = faces[i];
+            const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
+            t.tf_cells.push_back(L);
+            t.tf_cells.push_back(R);
+            for (int d = 0; d < 3; d++) t.tf_normal.push_back(d < dim ? m->face_normal[3 * (size_t)f + d] : 0.0);
+            for (int q = 0; q < 6; q++) t.tf_fdx.push_back(h.fdx[6 * (size_t)f + q]);
+            if (local[L] >= 0) lists[local[L]].push_back((uint16_t)i);
+            if (local[R] >= 0) lists[local[R]].push_back((uint16_t)(i | 0x8000));
+        }
+        for (int j = cb; j < ce; j++) {
+            t.tc_fptr[j + 1] = t.tc_fptr[j] + (int)lists[j - cb].size();
+            t.tc_face.insert(t.tc_face.end(), lists[j - cb].begin(), lists[j - cb].end());
+            local[t.cells[j]] = -1;
+        }
+        t.face_ptr.push_back((int32_t)(t.tf_cells.size() / 2));
+    }
+    return t;
 }
 
 inline HostMesh build_host_mesh(const abl_mesh_desc* m, bool need_cgrad, bool need_fgrad) {

@@ -330,6 +330,11 @@ class FiniteVolumeSolver:
         """F += RHS(U) with device pointers (e.g. torch tensors' data_ptr()), enqueued on `stream`."""
         L.check(L.lib.abl_fv_rhs(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(F_ptr), precision, C.c_void_p(stream)), "abl_fv_rhs")
 
+    def UpdateAux(self, locX: np.ndarray):
+        """Recompute the aux fields (T, u, Y) from host state locX (CellSolver::UpdateAuxFields)."""
+        x = np.ascontiguousarray(locX, dtype=np.float64)
+        L.check(L.lib.abl_fv_update_aux_host(self.handle, L.dptr(x)), "abl_fv_update_aux_host")
+
     def GetAux(self) -> np.ndarray:
         a = np.zeros((self.n_cells, self.naux))
         L.check(L.lib.abl_fv_get_aux(self.handle, L.dptr(a)))
@@ -341,6 +346,18 @@ class FiniteVolumeSolver:
 
     def Status(self) -> int:
         return L.lib.abl_fv_status(self.handle)
+
+    def Profile(self, enable: bool = True):
+        L.check(L.lib.abl_fv_profile(self.handle, int(enable)))
+
+    def ProfileRead(self) -> dict:
+        """Per-kernel device milliseconds of the last ComputeRHS* call (profiling must be on)."""
+        n = C.c_int32()
+        ms = (C.c_float * 8)()
+        names = C.create_string_buffer(32 * 8)
+        L.check(L.lib.abl_fv_profile_read(self.handle, C.byref(n), ms, names))
+        raw = names.raw
+        return {raw[32 * i:32 * (i + 1)].split(b"\0")[0].decode(): float(ms[i]) for i in range(n.value)}
 
     def LaunchCount(self, precision: int = L.PRECISION_FP64) -> int:
         n = C.c_int32()

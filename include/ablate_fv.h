@@ -103,6 +103,9 @@ extern "C" {
 /* precision of abl_fv_rhs */
 #define ABL_PRECISION_FP64 0
 #define ABL_PRECISION_MIXED 1 /* FP32 reconstruction/flux arithmetic, FP64 e=E/rho-|u|^2/2, T solve and accumulation */
+/* or'ed into the precision argument of abl_fv_rhs: F = RHS(U) instead of F += RHS(U) (for a caller
+ * whose residual vector holds nothing else; saves reading F) */
+#define ABL_RHS_OVERWRITE 0x100
 
 /* ---- descriptors ------------------------------------------------------------------------------ */
 /* One rank's local mesh: what DMPlex + DMPlexComputeGeometryFVM hold for the FV solver.
@@ -179,12 +182,22 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
 /* Same with host pointers (the plain PETSc Vec case): copies U in, runs abl_fv_rhs, adds into F. */
 int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision);
 
-/* Aux fields (T, u, Y) of the last evaluation / set the temperature guess used by the next one. */
+/* Aux fields (T, u, Y). With the NASA-7 mixture EOS every abl_fv_rhs updates them (the resident T is
+ * also the next secant guess); with a perfect gas the RHS recomputes them on the fly and they are
+ * refreshed only by abl_fv_update_aux. set_aux sets the temperature guess used by the next update. */
+int abl_fv_update_aux(abl_fv* fv, const double* U_dev, void* stream);
+int abl_fv_update_aux_host(abl_fv* fv, const double* U_host);
 int abl_fv_get_aux(abl_fv* fv, double* aux_host);
 int abl_fv_set_aux(abl_fv* fv, const double* aux_host);
 
 /* Device status word accumulated since the last call: ABL_OK or the first ABL_ERR_* a kernel saw. */
 int abl_fv_status(abl_fv* fv);
+
+/* Per-kernel device timing of abl_fv_rhs: with profiling on, each call records CUDA events between its
+ * launches; profile_read returns the durations of the last call (n <= 7 entries, ms[i] and the kernel
+ * name in names[32*i], NUL-terminated). */
+int abl_fv_profile(abl_fv* fv, int enable);
+int abl_fv_profile_read(abl_fv* fv, int32_t* n, float* ms, char* names);
 
 /* Number of kernel launches one abl_fv_rhs call makes at `precision` (for launch accounting). */
 int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches);
