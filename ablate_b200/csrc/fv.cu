@@ -460,11 +460,17 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         }
         // cell tiles for the fused flux kernel: the largest tile whose face fluxes fit in shared memory
         const int nc_ = 2 + h.dim + physics->n_species;
+        // tiles from the caller's cell order and from a Morton sort; keep the one that duplicates fewer faces
+        auto tiles_for = [&](int tile) {
+            Tiles a = build_tiles(h, mesh, tile, false);
+            Tiles b = build_tiles(h, mesh, tile, true);
+            return b.tf_cells.size() < a.tf_cells.size() ? b : a;
+        };
         int tile = 256;
-        Tiles tl = build_tiles(h, mesh, tile);
+        Tiles tl = tiles_for(tile);
         while ((size_t)tl.max_faces * nc_ * sizeof(double) > 200 * 1024 && tile > 16) {
             tile /= 2;
-            tl = build_tiles(h, mesh, tile);
+            tl = tiles_for(tile);
         }
         fv->tile_smem = (int)((size_t)std::max(tl.max_faces, 1) * nc_ * sizeof(double));
         fv->tile_cell_ptr.upload(tl.cell_ptr.data(), tl.cell_ptr.size());

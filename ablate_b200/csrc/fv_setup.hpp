@@ -131,7 +131,9 @@ inline uint64_t morton_spread(uint64_t x, int dim) {
     return r;
 }
 
-inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cells) {
+// morton = false keeps the caller's own cell order (compact when the DM was permuted along a
+// space-filling curve); true sorts owned cells by the Morton code of their centroids.
+inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cells, bool morton = true) {
     Tiles t;
     const int dim = h.dim;
     std::vector<int32_t> owned;
@@ -144,6 +146,7 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             hi[d] = std::max(hi[d], m->cell_centroid[3 * (size_t)c + d]);
         }
     const int bits = dim == 1 ? 62 : (dim == 2 ? 31 : 21);
+    (void)bits;
     const double scale = std::ldexp(1.0, bits) - 1.0;
     std::vector<std::pair<uint64_t, int32_t>> keyed(owned.size());
     for (size_t i = 0; i < owned.size(); i++) {
@@ -154,7 +157,7 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             const double u = span > 0 ? (m->cell_centroid[3 * (size_t)c + d] - lo[d]) / span : 0.0;
             key |= morton_spread((uint64_t)(u * scale), dim) << d;
         }
-        keyed[i] = {key, c};
+        keyed[i] = {morton ? key : (uint64_t)i, c};
     }
     std::sort(keyed.begin(), keyed.end());
     const int n = (int)keyed.size();

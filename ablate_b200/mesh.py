@@ -6,7 +6,10 @@ directions or, on non-periodic sides, one FV ghost cell behind every boundary fa
 and its volume the interior cell's, as ``DMPlexComputeGeometryFVM`` sets them). Support order is
 (interior, ghost) with the area-weighted normal pointing from the first to the second cell.
 
-Cells are numbered x-fastest; ghost cells follow the interior cells.
+Cells are numbered x-fastest (``order="natural"``, DMPlexCreateBoxMesh's order) or along a Morton
+curve (``order="morton"``: the numbering a DMPlexPermute with a space-filling-curve ordering gives,
+which makes every compact block of cells contiguous in memory); faces follow their left cell. Ghost
+cells follow the interior cells.
 """
 from __future__ import annotations
 
@@ -49,7 +52,16 @@ class Mesh:
                           L.dptr(cv), L.u8ptr(ck), L.dptr(fs) if fs is not None else None)
 
 
-def box_mesh(shape, lower=None, upper=None, periodic=None) -> Mesh:
+def _morton_keys(idx: np.ndarray, dim: int) -> np.ndarray:
+    """Interleave the bits of the integer cell coordinates idx[a] (a < dim) into one key per cell."""
+    key = np.zeros(idx.shape[1], dtype=np.uint64)
+    for b in range(21):
+        for a in range(dim):
+            key |= ((idx[a].astype(np.uint64) >> np.uint64(b)) & np.uint64(1)) << np.uint64(b * dim + a)
+    return key
+
+
+def box_mesh(shape, lower=None, upper=None, periodic=None, order: str = "natural") -> Mesh:
     shape = tuple(int(n) for n in shape)
     dim = len(shape)
     if dim not in (1, 2, 3) or min(shape) < 1:
@@ -122,6 +134,24 @@ def box_mesh(shape, lower=None, upper=None, periodic=None) -> Mesh:
     face_normal = np.concatenate(fns)
     face_centroid = np.concatenate(fcents)
     face_shift = np.concatenate(fshifts)
+    if order == "morton":
+        # renumber interior cells along the Morton curve, then sort faces by their left cell
+        key = _morton_keys(idx, dim)
+        perm = np.argsort(key, kind="stable")          # new -> old
+        rank = np.empty(n_int, np.int64)
+        rank[perm] = np.arange(n_int)                   # old -> new
+        cc = cc[perm]
+        fc = face_cells.astype(np.int64)
+        interior = fc < n_int
+        fc[interior] = rank[fc[interior]]
+        fo = np.lexsort((fc[:, 1], fc[:, 0]))
+        face_cells = fc[fo].astype(np.int32)
+        face_normal = face_normal[fo]
+        face_centroid = face_centroid[fo]
+        face_shift = face_shift[fo]
+        # ghost cells keep their creation order; their interior partners were renumbered above
+    elif order != "natural":
+        raise ValueError("order must be 'natural' or 'morton'")
     if n_ghost:
         cc = np.concatenate([cc] + ghost_cent)
     nc = n_int + n_ghost

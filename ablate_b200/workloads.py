@@ -1,6 +1,8 @@
 """Seeded synthetic workloads with the shapes of the benchmark configurations.
 
-No dataset is involved: every mesh and initial state is generated here from a fixed seed.
+No dataset is involved: every mesh and initial state is generated here from a fixed seed. Meshes
+are numbered along a Morton curve by default (the order a DMPlexPermute with a space-filling-curve
+ordering gives at setup); ``order="natural"`` gives DMPlexCreateBoxMesh's x-fastest numbering.
 
 * ``sod2d``   2D Euler, perfect gas (gamma 1.4, R 287), n x n quads on [0,1]^2 with outflow ghost
               cells; Sod jump at x = 0.5 (rho 1 / 0.125, p 1e5 / 1e4, u = 0) times seeded Gaussian
@@ -50,8 +52,8 @@ def fill_outflow_ghosts(mesh: Mesh, U: np.ndarray) -> None:
         U[g] = U[ghost_interior_map(mesh)]
 
 
-def sod2d(n: int = 256, seed: int = 20261203) -> Workload:
-    mesh = box_mesh((n, n))
+def sod2d(n: int = 256, seed: int = 20261203, order: str = "morton") -> Workload:
+    mesh = box_mesh((n, n), order=order)
     rng = np.random.default_rng(seed)
     gamma, R = 1.4, 287.0
     x = mesh.cell_centroid[:, 0]
@@ -94,8 +96,8 @@ def tgv_state(mesh: Mesh, gamma=1.4, R=287.0, mach=0.3, T0=300.0, p0=101325.0, n
     return U
 
 
-def tgv3d(n: int = 128, seed: int = 20261204) -> Workload:
-    mesh = box_mesh((n, n, n), periodic=(True, True, True))
+def tgv3d(n: int = 128, seed: int = 20261204, order: str = "morton") -> Workload:
+    mesh = box_mesh((n, n, n), periodic=(True, True, True), order=order)
     gamma, R = 1.4, 287.0
     U = tgv_state(mesh, gamma, R, seed=seed)
     mu, pr = 1.8e-5, 0.72
@@ -161,8 +163,8 @@ def mixture_state(eos: fv.TChem, rho, vel, T, Y):
     return U
 
 
-def shear3d(n: int = 256, ns: int = 5, seed: int = 20261205, diffusion: bool = False) -> Workload:
-    mesh = box_mesh((n, n, n), periodic=(True, False, True))
+def shear3d(n: int = 256, ns: int = 5, seed: int = 20261205, diffusion: bool = False, order: str = "morton") -> Workload:
+    mesh = box_mesh((n, n, n), periodic=(True, False, True), order=order)
     rng = np.random.default_rng(seed)
     eos = synthetic_mixture(ns, seed + 1)
     x, y, z = (mesh.cell_centroid[:, d] for d in range(3))

@@ -39,6 +39,10 @@ def case(name: str) -> Workload:
         return workloads.tgv3d(8)
     if name == "tgv3d_mixed_check":
         return workloads.tgv3d(16)
+    if name == "tgv3d_natural_order":
+        return workloads.tgv3d(8, order="natural")
+    if name == "sod2d_natural_order":
+        return workloads.sod2d(16, order="natural")
     if name.startswith("box2d_"):
         # 2D with ghost boundaries, LSQ, the limiter/flux named in the case
         _, flux, lim, tr = name.split("_")
@@ -82,6 +86,8 @@ def case(name: str) -> Workload:
 
 CASES = [
     "sod2d_ausm_upwind",
+    "sod2d_natural_order",
+    "tgv3d_natural_order",
     "box1d_riemann_upwind",
     "tgv3d_ausmpup_lsq_minmod_visc",
     "box2d_ausm_upwind_none",
