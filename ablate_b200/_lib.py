@@ -81,6 +81,8 @@ SIGNATURES = {
     "abl_fv_profile_read": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_float), C.c_char_p]),
     "abl_flux_calculator_batch": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double, C.c_int64] + [_dp] * 10 + [_ip]),
     "abl_eos_batch": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, _dp, _dp, _dp]),
+    "abl_eos_batch_noalloc": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
 }
 
 

@@ -393,6 +393,31 @@ int status_to_code(int bits) {
 
 }  // namespace
 
+// ---- allocation-free EOS batch ----------------------------------------------------------------------
+// Scratch of abl_eos_batch_noalloc: the NASA-7 tables the kernel reads (T_mid + 14 coefficients, molar
+// mass, 1/molar mass, reference enthalpy per species) followed by the status word. 16 KiB, held by every
+// GPU that loads this library until the process exits; 64 species need 9,216 bytes.
+constexpr int kNoAllocMaxSpecies = 64;
+constexpr size_t kNoAllocScratchBytes = 16384;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[256] = {};
+
+// Device address of g_noalloc_scratch on the current device, resolved once per device (host code
+// cannot use the symbol itself: on the host it names a stand-in, not device memory).
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= 256) throw std::invalid_argument("device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr) throw AblError(ABL_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_address[device] = ptr;
+    }
+    return static_cast<unsigned char*>(g_noalloc_address[device]);
+}
+
 // =================================================================================================
 extern "C" {
 
@@ -725,6 +750,65 @@ int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_
         if (psz > 0) ABL_CUDA(cudaMemcpy(out, o.p, (size_t)n * psz * sizeof(double), cudaMemcpyDeviceToHost));
         int bits = 0;
         ABL_CUDA(cudaMemcpy(&bits, st.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (bits & kStatusEos) throw AblError(ABL_ERR_EOS_NOT_CONVERGED, "temperature iteration did not converge");
+    });
+}
+
+int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved_dev, const double* T_dev,
+                          double* out_dev, void* stream) {
+    return guarded([&] {
+        validate_physics(physics);
+        if (dim < 1 || dim > 3) throw std::invalid_argument("dim must be 1, 2 or 3");
+        if (property < ABL_PROP_PRESSURE || property > ABL_PROP_DENSITY) throw std::invalid_argument("unknown property");
+        if (n < 0 || (n > 0 && (!conserved_dev || !out_dev))) throw std::invalid_argument("NULL argument");
+        const int ns = physics->n_species;
+        if (ns > kNoAllocMaxSpecies)
+            throw std::invalid_argument("abl_eos_batch_noalloc: " + std::to_string(ns) + " species exceed the " +
+                                        std::to_string(kNoAllocMaxSpecies) + " its static scratch holds");
+        if (n == 0) return;
+        int device = 0;
+        ABL_CUDA(cudaGetDevice(&device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        unsigned char* scratch = noalloc_scratch(device);
+        // layout: nasa7 [ns][15] | mw [ns] | 1/mw [ns] | h_ref [ns] | status (int)
+        double* d_nasa7 = reinterpret_cast<double*>(scratch);
+        double* d_mw = d_nasa7 + 15 * kNoAllocMaxSpecies;
+        double* d_imw = d_mw + kNoAllocMaxSpecies;
+        double* d_href = d_imw + kNoAllocMaxSpecies;
+        int* d_status = reinterpret_cast<int*>(d_href + kNoAllocMaxSpecies);
+        static_assert((15 + 3) * kNoAllocMaxSpecies * sizeof(double) + sizeof(int) <= kNoAllocScratchBytes, "scratch too small");
+        Phys P = make_phys(physics);
+        if (physics->eos == ABL_EOS_NASA7) {
+            std::vector<double> tables(18 * (size_t)ns);
+            for (int k = 0; k < ns; k++) {
+                if (!(physics->mw[k] > 0)) throw std::invalid_argument("molar mass must be positive");
+                tables[15 * (size_t)ns + k] = physics->mw[k];
+                tables[16 * (size_t)ns + k] = 1.0 / physics->mw[k];
+                tables[17 * (size_t)ns + k] = host_h_molar(physics->nasa7 + 15 * k, kTref) / physics->mw[k];
+            }
+            std::memcpy(tables.data(), physics->nasa7, 15 * (size_t)ns * sizeof(double));
+            // pageable host source: the copy is staged before cudaMemcpyAsync returns, so `tables` may go
+            ABL_CUDA(cudaMemcpyAsync(d_nasa7, tables.data(), 15 * (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s));
+            ABL_CUDA(cudaMemcpyAsync(d_mw, tables.data() + 15 * (size_t)ns, (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s));
+            ABL_CUDA(cudaMemcpyAsync(d_imw, tables.data() + 16 * (size_t)ns, (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s));
+            ABL_CUDA(cudaMemcpyAsync(d_href, tables.data() + 17 * (size_t)ns, (size_t)ns * sizeof(double), cudaMemcpyHostToDevice, s));
+            P.nasa7 = d_nasa7;
+            P.mw = d_mw;
+            P.inv_mw = d_imw;
+            P.href = d_href;
+        }
+        // the status word is the one scratch entry read before it is written: clear it every call
+        ABL_CUDA(cudaMemsetAsync(d_status, 0, sizeof(int), s));
+        const unsigned nb = blocks_for(n, 128);
+        switch (dim) {
+            case 1: k_eos_batch<1><<<nb, 128, 0, s>>>(P, ns, property, n, conserved_dev, T_dev, out_dev, d_status); break;
+            case 2: k_eos_batch<2><<<nb, 128, 0, s>>>(P, ns, property, n, conserved_dev, T_dev, out_dev, d_status); break;
+            default: k_eos_batch<3><<<nb, 128, 0, s>>>(P, ns, property, n, conserved_dev, T_dev, out_dev, d_status); break;
+        }
+        check_launch();
+        int bits = 0;
+        ABL_CUDA(cudaMemcpyAsync(&bits, d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
+        ABL_CUDA(cudaStreamSynchronize(s));
         if (bits & kStatusEos) throw AblError(ABL_ERR_EOS_NOT_CONVERGED, "temperature iteration did not converge");
     });
 }

@@ -216,6 +216,21 @@ int abl_flux_calculator_batch(int kind, double minf, double pgs_alpha, double ga
 int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved,
                   const double* T_in, double* out);
 
+/* Allocation-free variant of abl_eos_batch for states already on the device. No counterpart in the
+ * reference. abl_eos_batch copies host arrays and the species tables into device buffers it allocates
+ * and frees on every call; a caller whose device memory is reserved by a pool allocator (PETSc's or
+ * PyTorch's) may be unable to allocate at all, and one evaluating properties inside a time step cannot
+ * afford the device-wide synchronisation every cudaFree implies. This entry point calls no cudaMalloc,
+ * cudaFree or allocating library routine: conserved_dev[n][nc], T_dev[n] (or NULL) and out_dev[n][property
+ * size] are the caller's device buffers, and the NASA-7 tables and the status word live in a 16 KiB
+ * file-scope device array of the library (held by every GPU that loads it until exit), which limits
+ * n_species to 64. Work is ordered on `stream`; the call waits for it to finish to return the status.
+ * The first call on a device resolves the array's device address and should come before any stream
+ * capture. Every call reuses the same array: calls that overlap on the GPU (other streams, other host
+ * threads) race on it. */
+int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved_dev,
+                          const double* T_dev, double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
