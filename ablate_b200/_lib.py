@@ -71,6 +71,8 @@ SIGNATURES = {
     "abl_fv_sizes": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "abl_fv_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
+    "abl_fv_jvp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_jvp_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp]),
     "abl_fv_update_aux": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_update_aux_host": (C.c_int, [C.c_void_p, _dp]),
     "abl_fv_get_aux": (C.c_int, [C.c_void_p, _dp]),

@@ -54,14 +54,16 @@ def build_product(force: bool = False, verbose: bool = False) -> Path:
     LIBDIR.mkdir(parents=True, exist_ok=True)
     objdir = LIBDIR / "obj"
     objdir.mkdir(exist_ok=True)
-    objs = []
-    for src in sources:
-        obj = objdir / (src.stem + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
-        if verbose:
+    objs = [str(objdir / (src.stem + ".o")) for src in sources]
+    cmds = [[_nvcc(), *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", obj] for src, obj in zip(sources, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+    # one nvcc per translation unit, in parallel
+    procs = [subprocess.Popen(cmd) for cmd in cmds]
+    codes = [p.wait() for p in procs]
+    if any(codes):
+        raise subprocess.CalledProcessError(max(codes), cmds[codes.index(max(codes))])
     cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(LIB), "-lcudart"]
     subprocess.run(cmd, check=True)
     return LIB

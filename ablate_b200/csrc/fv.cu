@@ -11,102 +11,16 @@
 #include <string>
 #include <vector>
 
-#include "fv_kernels.cuh"
+#include "fv_handle.hpp"
 #include "fv_setup.hpp"
 
 namespace abl {
-
 thread_local std::string g_last_error;
-
-struct AblError : std::runtime_error {
-    int code;
-    AblError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define ABL_CUDA(call)                                                                                           \
-    do {                                                                                                         \
-        cudaError_t e_ = (call);                                                                                 \
-        if (e_ != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-    void alloc(size_t count) {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = count;
-        if (count == 0) return;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            throw AblError(e == cudaErrorMemoryAllocation ? ABL_ERR_OUT_OF_MEMORY : ABL_ERR_CUDA,
-                           std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        }
-    }
-    void upload(const T* h, size_t count) {
-        alloc(count);
-        if (count) ABL_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
-    }
-    void zero() {
-        if (n) ABL_CUDA(cudaMemset(p, 0, n * sizeof(T)));
-    }
-};
-
 }  // namespace abl
 
 using namespace abl;
 
-struct abl_fv {
-    int device = 0;
-    int dim = 0, ns = 0, nc = 0, naux = 0;
-    int n_cells = 0, n_faces = 0, n_flux_faces = 0;
-    Phys phys{};
-    DevMesh mesh{};
-    // resident mesh + geometry
-    DevBuf<int2> face_cells;
-    DevBuf<uint8_t> kind, cone_side, face_boundary;
-    DevBuf<int> cone_ptr, cone_face, cone_nbr;
-    DevBuf<double> fdx, ivol, cgrad, fgrad;
-    DevBuf<double> nasa7, mw, inv_mw, href;
-    // tiles
-    DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
-    DevBuf<int2> tf_cells;
-    DevBuf<double> tf_normal, tf_fdx;
-    DevBuf<uint16_t> tc_face;
-    int tile_smem = 0;
-    // optional per-kernel timing of the last abl_fv_rhs call
-    bool profile = false;
-    int n_marks = 0;
-    cudaEvent_t marks[8] = {};
-    const char* mark_names[8] = {};
-    // work buffers
-    DevBuf<double> aux;
-    DevBuf<double> grad64, agrad64;
-    DevBuf<float> grad32, agrad32;
-    DevBuf<int> status;
-    // host-pointer path
-    DevBuf<double> hU, hF;
-    bool need_aux = false, need_state_grad = false, need_aux_grad = false;
-};
-
 namespace {
-
-// record a timing mark (event) before the next launch when profiling is on
-void mark(abl_fv* fv, const char* name, cudaStream_t s) {
-    if (!fv->profile || fv->n_marks >= 8) return;
-    if (!fv->marks[fv->n_marks]) ABL_CUDA(cudaEventCreate(&fv->marks[fv->n_marks]));
-    ABL_CUDA(cudaEventRecord(fv->marks[fv->n_marks], s));
-    fv->mark_names[fv->n_marks] = name;
-    fv->n_marks++;
-}
 
 int fail(const AblError& e) {
     g_last_error = e.what();
@@ -133,12 +47,6 @@ int guarded(F&& fn) {
     }
 }
 
-inline unsigned blocks_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
-
-void check_launch() {
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-}
 
 // host NASA-7 molar enthalpy, same polynomial as the device
 double host_h_molar(const double* c, double T) {
@@ -204,57 +112,6 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
 }
 
 // ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
-template <int DIM, int NS, class G>
-void launch_tile(abl_fv* fv, const double* U, const G* grad, const G* agrad, double* F, int overwrite, cudaStream_t s) {
-    auto kern = k_tile_flux<DIM, NS, G>;
-    static thread_local int configured = -1;
-    if (configured != fv->tile_smem) {
-        ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, fv->tile_smem));
-        configured = fv->tile_smem;
-    }
-    kern<<<fv->mesh.n_tiles, 128, fv->tile_smem, s>>>(fv->mesh, fv->phys, U, fv->aux.p, grad, agrad, F, overwrite, fv->status.p);
-    check_launch();
-}
-
-template <int DIM, int NS>
-void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
-    const DevMesh& M = fv->mesh;
-    const Phys& P = fv->phys;
-    fv->n_marks = 0;
-    if (fv->need_aux) {
-        mark(fv, "k_aux", s);
-        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, P, U, fv->aux.p, fv->status.p);
-        check_launch();
-    }
-    const bool grads = fv->need_state_grad || fv->need_aux_grad;
-    if (precision == ABL_PRECISION_MIXED) {
-        if (grads) {
-            mark(fv, "k_gradient", s);
-            k_gradient<DIM, NS, float><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad32.p, fv->agrad32.p,
-                                                                                   fv->need_state_grad, fv->need_aux_grad);
-            check_launch();
-        }
-        mark(fv, "k_tile_flux", s);
-        if (M.n_tiles > 0) launch_tile<DIM, NS, float>(fv, U, fv->grad32.p, fv->agrad32.p, F, overwrite, s);
-    } else {
-        if (grads) {
-            mark(fv, "k_gradient", s);
-            k_gradient<DIM, NS, double><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p,
-                                                                                    fv->need_state_grad, fv->need_aux_grad);
-            check_launch();
-        }
-        mark(fv, "k_tile_flux", s);
-        if (M.n_tiles > 0) launch_tile<DIM, NS, double>(fv, U, fv->grad64.p, fv->agrad64.p, F, overwrite, s);
-    }
-    mark(fv, "end", s);
-}
-
-template <int DIM, int NS>
-void run_aux(abl_fv* fv, const double* U, cudaStream_t s) {
-    k_aux<DIM, NS><<<blocks_for(fv->mesh.n_cells, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->aux.p, fv->status.p);
-    check_launch();
-}
-
 #define ABL_DISPATCH(fv, FN, ...)                                                                                                  \
     do {                                                                                                                           \
         switch ((fv)->dim * 100 + (fv)->ns) {                                                                                      \
@@ -271,6 +128,10 @@ void run_aux(abl_fv* fv, const double* U, cudaStream_t s) {
 
 void dispatch_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
     ABL_DISPATCH(fv, run_rhs, U, F, precision, overwrite, s);
+}
+
+void dispatch_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* dF, cudaStream_t s) {
+    ABL_DISPATCH(fv, run_jvp, U, dU, F, dF, s);
 }
 
 bool rhs_supported(int dim, int ns) {
@@ -473,10 +334,17 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->face_cells.upload(reinterpret_cast<const int2*>(h.face_cells.data()), h.n_faces);
         fv->kind.upload(h.kind.data(), h.kind.size());
         fv->cone_ptr.upload(h.cone_ptr.data(), h.cone_ptr.size());
-        fv->cone_face.upload(h.cone_face.data(), h.cone_face.size());
-        fv->cone_nbr.upload(h.cone_nbr.data(), h.cone_nbr.size());
-        fv->cone_side.upload(h.cone_side.data(), h.cone_side.size());
-        fv->face_boundary.upload(h.face_boundary.data(), h.face_boundary.size());
+        {
+            // cone entry: (face, neighbour | side << 31 | boundary face << 30)
+            if (h.n_cells >= (1 << 30)) throw std::invalid_argument("too many cells for the packed cone");
+            std::vector<int2> cone(h.cone_face.size());
+            for (size_t i = 0; i < cone.size(); i++) {
+                const int f = h.cone_face[i];
+                cone[i].x = f;
+                cone[i].y = h.cone_nbr[i] | (h.cone_side[i] ? kConeSide : 0) | (h.face_boundary[f] ? kConeBoundary : 0);
+            }
+            fv->cone.upload(cone.data(), cone.size());
+        }
         fv->fdx.upload(h.fdx.data(), h.fdx.size());
         {
             std::vector<double> iv(h.n_cells);
@@ -516,12 +384,12 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             ABL_CUDA(cudaMemcpy(fv->aux.p, a0.data(), a0.size() * sizeof(double), cudaMemcpyHostToDevice));
         }
         if (lsq) {
-            fv->grad64.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
-            fv->grad32.alloc((size_t)fv->n_cells * fv->nc * fv->dim);
+            fv->grad64.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 2));
+            fv->grad32.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 4));
         }
         if (dif) {
-            fv->agrad64.alloc((size_t)fv->n_cells * fv->naux * fv->dim);
-            fv->agrad32.alloc((size_t)fv->n_cells * fv->naux * fv->dim);
+            fv->agrad64.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 2));
+            fv->agrad32.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 4));
         }
         fv->status.alloc(1);
         fv->status.zero();
@@ -534,10 +402,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.face_cells = fv->face_cells.p;
         M.kind = fv->kind.p;
         M.cone_ptr = fv->cone_ptr.p;
-        M.cone_face = fv->cone_face.p;
-        M.cone_nbr = fv->cone_nbr.p;
-        M.cone_side = fv->cone_side.p;
-        M.face_boundary = fv->face_boundary.p;
+        M.cone = fv->cone.p;
         M.fdx = fv->fdx.p;
         M.ivol = fv->ivol.p;
         M.cgrad = fv->cgrad.p;
@@ -605,6 +470,38 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
         if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
         ABL_CUDA(cudaSetDevice(fv->device));
         dispatch_rhs(fv, U_dev, F_dev, precision, overwrite, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_jvp(abl_fv* fv, double time, const double* U_dev, const double* dU_dev, double* F_dev, double* dF_dev, void* stream) {
+    (void)time;
+    return guarded([&] {
+        if (!fv || !U_dev || !dU_dev || !dF_dev) throw std::invalid_argument("abl_fv_jvp: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        // value + tangent gradient pairs, allocated on first use
+        if (fv->need_state_grad && fv->gradD.n == 0) fv->gradD.alloc((size_t)fv->n_cells * fv->nc * fv->dim * 2);
+        if (fv->need_aux_grad && fv->agradD.n == 0) fv->agradD.alloc((size_t)fv->n_cells * fv->naux * fv->dim * 2);
+        dispatch_jvp(fv, U_dev, dU_dev, F_dev, dF_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double* dU_host, double* F_host, double* dF_host) {
+    return guarded([&] {
+        if (!fv || !U_host || !dU_host || !dF_host) throw std::invalid_argument("abl_fv_jvp_host: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->hU.n != n) fv->hU.alloc(n);
+        if (fv->hdU.n != n) fv->hdU.alloc(n);
+        if (fv->hdF.n != n) fv->hdF.alloc(n);
+        if (F_host && fv->hF.n != n) fv->hF.alloc(n);
+        ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        ABL_CUDA(cudaMemcpy(fv->hdU.p, dU_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        ABL_CUDA(cudaMemcpy(fv->hdF.p, dF_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        if (F_host) ABL_CUDA(cudaMemcpy(fv->hF.p, F_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        int rc = abl_fv_jvp(fv, time, fv->hU.p, fv->hdU.p, F_host ? fv->hF.p : nullptr, fv->hdF.p, nullptr);
+        if (rc != ABL_OK) throw AblError(rc, g_last_error);
+        ABL_CUDA(cudaMemcpy(dF_host, fv->hdF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (F_host) ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }
 

@@ -1,0 +1,121 @@
+// fv_handle.hpp -- host-side state of one abl_fv handle and the helpers the ABI and launch code share.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "fv_kernels.cuh"
+
+namespace abl {
+
+extern thread_local std::string g_last_error;
+
+struct AblError : std::runtime_error {
+    int code;
+    AblError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define ABL_CUDA(call)                                                                                           \
+    do {                                                                                                         \
+        cudaError_t e_ = (call);                                                                                 \
+        if (e_ != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t count) {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = count;
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw AblError(e == cudaErrorMemoryAllocation ? ABL_ERR_OUT_OF_MEMORY : ABL_ERR_CUDA,
+                           std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+    }
+    void upload(const T* h, size_t count) {
+        alloc(count);
+        if (count) ABL_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    void zero() {
+        if (n) ABL_CUDA(cudaMemset(p, 0, n * sizeof(T)));
+    }
+};
+
+inline unsigned blocks_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+inline void check_launch() {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw AblError(ABL_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+// gradient rows are padded to whole 16-byte vectors (see GradRows in fv_kernels.cuh)
+inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+}  // namespace abl
+
+struct abl_fv {
+    int device = 0;
+    int dim = 0, ns = 0, nc = 0, naux = 0;
+    int n_cells = 0, n_faces = 0, n_flux_faces = 0;
+    abl::Phys phys{};
+    abl::DevMesh mesh{};
+    // resident mesh + geometry
+    abl::DevBuf<int2> face_cells, cone;
+    abl::DevBuf<uint8_t> kind;
+    abl::DevBuf<int> cone_ptr;
+    abl::DevBuf<double> fdx, ivol, cgrad, fgrad;
+    abl::DevBuf<double> nasa7, mw, inv_mw, href;
+    // tiles
+    abl::DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
+    abl::DevBuf<int2> tf_cells;
+    abl::DevBuf<double> tf_normal, tf_fdx;
+    abl::DevBuf<uint16_t> tc_face;
+    int tile_smem = 0;
+    // optional per-kernel timing of the last evaluation
+    bool profile = false;
+    int n_marks = 0;
+    cudaEvent_t marks[8] = {};
+    const char* mark_names[8] = {};
+    // work buffers: aux, gradients (FP64, FP32, and value+tangent pairs for the tangent kernels)
+    abl::DevBuf<double> aux;
+    abl::DevBuf<double> grad64, agrad64, gradD, agradD;
+    abl::DevBuf<float> grad32, agrad32;
+    abl::DevBuf<int> status;
+    // host-pointer paths
+    abl::DevBuf<double> hU, hF, hdU, hdF;
+    bool need_aux = false, need_state_grad = false, need_aux_grad = false;
+};
+
+namespace abl {
+
+// record a timing mark (event) before the next launch when profiling is on
+inline void mark(abl_fv* fv, const char* name, cudaStream_t s) {
+    if (!fv->profile || fv->n_marks >= 8) return;
+    if (!fv->marks[fv->n_marks]) ABL_CUDA(cudaEventCreate(&fv->marks[fv->n_marks]));
+    ABL_CUDA(cudaEventRecord(fv->marks[fv->n_marks], s));
+    fv->mark_names[fv->n_marks] = name;
+    fv->n_marks++;
+}
+
+// launch sequences, explicitly instantiated per (DIM, NS) in fv_inst_*.cu
+template <int DIM, int NS>
+void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s);
+template <int DIM, int NS>
+void run_aux(abl_fv* fv, const double* U, cudaStream_t s);
+template <int DIM, int NS>
+void run_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* dF, cudaStream_t s);
+
+}  // namespace abl

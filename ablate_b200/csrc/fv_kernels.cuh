@@ -30,10 +30,8 @@ struct DevMesh {
     const int2* face_cells;
     const uint8_t* kind;
     const int* cone_ptr;
-    const int* cone_face;
-    const int* cone_nbr;
-    const uint8_t* cone_side;
-    const uint8_t* face_boundary;
+    // cone entry of a cell: x = face, y = neighbour | side << 31 | (face touches a boundary ghost) << 30
+    const int2* cone;
     const double* fdx;     // [nf][2][3] face centroid - side cell centroid (cell's own frame)
     const double* ivol;    // [nc] 1 / volume
     const double* cgrad;   // [nf][2][3]
@@ -57,33 +55,121 @@ struct Dims {
     static constexpr int NA = 1 + DIM + NS;  // aux components per cell (T, u, Y)
 };
 
+// Row strides of the per-cell gradient arrays, padded to whole 16-byte vectors
+template <int DIM, int NS, class G>
+struct GradRows {
+    static constexpr int V = 16 / sizeof(G);  // elements per 16-byte vector
+    static constexpr int GS = ((Dims<DIM, NS>::NC * DIM + V - 1) / V) * V;
+    static constexpr int AS = ((Dims<DIM, NS>::NA * DIM + V - 1) / V) * V;
+};
+
+// minimum resident CTAs per SM for __launch_bounds__ (register budget per thread = 65536 / (128 * n)):
+// FP32 reconstruction fits 6 gradient CTAs, FP64 4, the value+tangent pairs of the tangent kernels 1
+template <int NS, class G>
+struct MinBlocks {
+    static constexpr int grad = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : (NS > 0 ? 3 : (sizeof(G) == 8 ? 4 : 6)));
+    static constexpr int tile = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : 3);
+};
+
+constexpr int kConeSide = int(1u << 31);
+constexpr int kConeBoundary = 1 << 30;
+constexpr int kConeNbr = (1 << 30) - 1;
+
+// load n elements of a 16-byte-aligned row with vector loads
+template <int N, class G>
+__device__ __forceinline__ void load_row(const G* __restrict__ p, G* out) {
+    if constexpr (std::is_same<G, Dual>::value) {
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+            out[i] = Dual(v.x, v.y);
+        }
+    } else if constexpr (sizeof(G) == 8) {
+#pragma unroll
+        for (int i = 0; i < N / 2; i++) {
+            const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+            out[2 * i] = v.x;
+            out[2 * i + 1] = v.y;
+        }
+        if constexpr (N % 2) out[N - 1] = __ldg(p + N - 1);
+    } else {
+#pragma unroll
+        for (int i = 0; i < N / 4; i++) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
+            out[4 * i] = v.x;
+            out[4 * i + 1] = v.y;
+            out[4 * i + 2] = v.z;
+            out[4 * i + 3] = v.w;
+        }
+#pragma unroll
+        for (int i = (N / 4) * 4; i < N; i++) out[i] = __ldg(p + i);
+    }
+}
+
 template <class G>
 __device__ __forceinline__ G big_value();
 template <>
 __device__ __forceinline__ double big_value<double>() { return DBL_MAX; }
 template <>
 __device__ __forceinline__ float big_value<float>() { return FLT_MAX; }
+template <>
+__device__ __forceinline__ Dual big_value<Dual>() { return Dual(DBL_MAX); }
 
-template <int DIM, int NS>
-__device__ __forceinline__ void load_state(const double* __restrict__ U, int c, double* u) {
+// scalar type of the state and fluxes for a gradient storage type: Dual in the tangent kernels,
+// double otherwise (the mixed path keeps the state in FP64)
+template <class G>
+using StateOf = typename std::conditional<std::is_same<G, Dual>::value, Dual, double>::type;
+
+template <class S, class G>
+__device__ __forceinline__ S to_state(G x) {
+    return static_cast<S>(x);
+}
+template <>
+__device__ __forceinline__ double to_state<double, Dual>(Dual x) {
+    return x.v;
+}
+
+// state row of cell c; a Dual state also reads the tangent row from dU
+template <int DIM, int NS, class S>
+__device__ __forceinline__ void load_state(const double* __restrict__ U, const double* __restrict__ dU, int c, S* u) {
     using D = Dims<DIM, NS>;
 #pragma unroll
-    for (int k = 0; k < D::NC; k++) u[k] = __ldg(U + (size_t)c * D::NC + k);
+    for (int k = 0; k < D::NC; k++) {
+        if constexpr (std::is_same<S, Dual>::value)
+            u[k] = Dual(__ldg(U + (size_t)c * D::NC + k), __ldg(dU + (size_t)c * D::NC + k));
+        else
+            u[k] = __ldg(U + (size_t)c * D::NC + k);
+    }
+}
+template <int DIM, int NS>
+__device__ __forceinline__ void load_state(const double* __restrict__ U, int c, double* u) {
+    load_state<DIM, NS, double>(U, nullptr, c, u);
 }
 
 // aux (T, u, Y) of one cell: from the resident aux array for the mixture EOS, recomputed from the
 // conserved state for a perfect gas (UpdateAuxTemperatureField / UpdateAuxVelocityField /
 // UpdateAuxMassFractionField: navierStokesTransport.cpp:534-558, speciesTransport.cpp:98-110)
-template <int DIM, int NS>
-__device__ __forceinline__ void cell_aux(const Phys& P, const double* u, const double* __restrict__ aux, int c, double* a) {
+template <int DIM, int NS, class S>
+__device__ __forceinline__ void cell_aux(const Phys& P, const S* u, const double* __restrict__ aux, int c, S* a) {
     using D = Dims<DIM, NS>;
     if (NS > 0 && P.eos == ABL_EOS_NASA7) {
+        if constexpr (std::is_same<S, Dual>::value) {
+            // tangent: T from the state (its derivative by the implicit-function theorem), the resident T as guess
+            bool ok = true;
+            a[0] = temperature<DIM, NS>(P, NS, u, __ldg(aux + (size_t)c * D::NA), &ok);
+            const S irho = rcp64(u[0]);
 #pragma unroll
-        for (int k = 0; k < D::NA; k++) a[k] = __ldg(aux + (size_t)c * D::NA + k);
+            for (int d = 0; d < DIM; d++) a[1 + d] = u[2 + d] * irho;
+#pragma unroll
+            for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
+        } else {
+#pragma unroll
+            for (int k = 0; k < D::NA; k++) a[k] = __ldg(aux + (size_t)c * D::NA + k);
+        }
         return;
     }
-    const double irho = rcp64(u[0]);
-    double ke = 0.0;
+    const S irho = rcp64(u[0]);
+    S ke = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
         a[1 + d] = u[2 + d] * irho;
@@ -114,30 +200,35 @@ __global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __
 }
 
 // ---------------------------------------------------------------------------------------------------
-template <int DIM, int NS, class G>
-__device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U, const double* uc,
-                                            G* g, int k0, int k1) {
+// limiter of one field (components k0..k1-1) of cell c with gradient g (DMPlexApplyLimiter_Internal,
+// cellInterpolant.cpp:282-328, and the cancel rule at :459-481)
+template <int DIM, int NS, class G, int LIM>
+__device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U,
+                                            const double* __restrict__ dU, const StateOf<G>* uc, G* g, int k0, int k1) {
     using D = Dims<DIM, NS>;
+    using S = StateOf<G>;
     G phi[D::NC];
 #pragma unroll
     for (int k = 0; k < D::NC; k++) phi[k] = big_value<G>();
+#pragma unroll 2
     for (int i = beg; i < end; i++) {
-        const int n = M.cone_nbr[i];
-        const int f = M.cone_face[i];
-        const int sc = M.cone_side[i];
+        const int2 ce = M.cone[i];
+        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
         // x_n - x_c = (x_f - x_c) - (x_f - x_n), each offset taken in its own cell's frame
         G v[DIM];
 #pragma unroll
         for (int d = 0; d < DIM; d++) v[d] = G(__ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d));
+        S un[D::NC];
+        load_state<DIM, NS, S>(U, dU, n, un);
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
             if (k < k0 || k >= k1) continue;
             G denom = 0;
 #pragma unroll
             for (int d = 0; d < DIM; d++) denom += g[k * DIM + d] * v[d];
-            const G diff = G(__ldg(U + (size_t)n * D::NC + k) - uc[k]);
+            const G diff = G(un[k] - uc[k]);
             const G flim = G(0.5) * diff * rcp64(denom);
-            phi[k] = pmin(phi[k], limiter<G>(P.limiter, flim));
+            phi[k] = pmin(phi[k], limiter_k<LIM, G>(P.limiter, flim));
         }
     }
     bool cancel = false;
@@ -158,71 +249,76 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
     }
 }
 
-template <int DIM, int NS, class G>
-__global__ void __launch_bounds__(128, (NS > 2 ? 3 : 6)) k_gradient(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
-                                                  G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux) {
+// One thread per cell: one pass over the cell's faces accumulates the LSQ gradient of the conserved
+// fields (non-boundary faces, cgrad weights) and of the aux fields (all faces, fgrad weights), a second
+// pass applies the limiter. Cells without a conserved-state gradient (boundary ghosts, outer halo) get
+// a zero row, so the flux kernel projects every cell without a branch.
+template <int DIM, int NS, class G, int LIM>
+__global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMesh M, Phys P, const double* __restrict__ U,
+                                                                    const double* __restrict__ dU, const double* __restrict__ aux,
+                                                                    G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux) {
     using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, G>;
+    using S = StateOf<G>;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= M.n_cells) return;
     const uint8_t kind = M.kind[c];
     const int beg = M.cone_ptr[c], end = M.cone_ptr[c + 1];
-    double uc[D::NC];
-    load_state<DIM, NS>(U, c, uc);
-    if (do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO)) {
-        G g[D::NC * DIM];
+    const bool state = do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO);
+    const bool auxg = do_aux && kind != ABL_CELL_HALO_OUTER;
+    const bool nasa = NS > 0 && P.eos == ABL_EOS_NASA7;
+    S uc[D::NC], ac[D::NA];
+    load_state<DIM, NS, S>(U, dU, c, uc);
+    if (auxg) cell_aux<DIM, NS>(P, uc, aux, c, ac);
+    G g[D::NC * DIM], ga[D::NA * DIM];
 #pragma unroll
-        for (int k = 0; k < D::NC * DIM; k++) g[k] = G(0);
+    for (int k = 0; k < D::NC * DIM; k++) g[k] = G(0);
+#pragma unroll
+    for (int k = 0; k < D::NA * DIM; k++) ga[k] = G(0);
+    if (state || auxg) {
+#pragma unroll 2
         for (int i = beg; i < end; i++) {
-            const int f = M.cone_face[i];
-            if (M.face_boundary[f]) continue;
-            const int n = M.cone_nbr[i];
-            const double* w = M.cgrad + 6 * (size_t)f + 3 * M.cone_side[i];
-            G wd[DIM];
+            const int2 ce = M.cone[i];
+            const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+            S un[D::NC];
+            if (state || !nasa || std::is_same<S, Dual>::value) load_state<DIM, NS, S>(U, dU, n, un);
+            if (state && !(ce.y & kConeBoundary)) {
+                G wd[DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(w + d));
+                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.cgrad + 6 * (size_t)f + 3 * sc + d));
 #pragma unroll
-            for (int k = 0; k < D::NC; k++) {
-                const G delta = G(__ldg(U + (size_t)n * D::NC + k) - uc[k]);
+                for (int k = 0; k < D::NC; k++) {
+                    const G delta = G(un[k] - uc[k]);
 #pragma unroll
-                for (int d = 0; d < DIM; d++) g[k * DIM + d] += wd[d] * delta;
+                    for (int d = 0; d < DIM; d++) g[k * DIM + d] += wd[d] * delta;
+                }
+            }
+            if (auxg) {
+                S an[D::NA];
+                cell_aux<DIM, NS>(P, un, aux, n, an);
+                G wd[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.fgrad + 6 * (size_t)f + 3 * sc + d));
+#pragma unroll
+                for (int k = 0; k < D::NA; k++) {
+                    const G delta = G(an[k] - ac[k]);
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) ga[k * DIM + d] += wd[d] * delta;
+                }
             }
         }
-        if (P.limiter != ABL_LIMITER_NONE) {
-            limit_field<DIM, NS, G>(M, P, beg, end, U, uc, g, 0, D::NE);
-            if (NS > 0) limit_field<DIM, NS, G>(M, P, beg, end, U, uc, g, D::NE, D::NC);
+        if (state && P.limiter != ABL_LIMITER_NONE) {
+            limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, 0, D::NE);
+            if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC);
         }
-        G* out = grad + (size_t)c * D::NC * DIM;
+    }
+    if (do_state) {
+        G* out = grad + (size_t)c * GR::GS;
 #pragma unroll
         for (int k = 0; k < D::NC * DIM; k++) out[k] = g[k];
     }
-    if (do_aux && kind != ABL_CELL_HALO_OUTER) {
-        double ac[D::NA];
-        cell_aux<DIM, NS>(P, uc, aux, c, ac);
-        G ga[D::NA * DIM];
-#pragma unroll
-        for (int k = 0; k < D::NA * DIM; k++) ga[k] = G(0);
-        for (int i = beg; i < end; i++) {
-            const int f = M.cone_face[i];
-            const int n = M.cone_nbr[i];
-            const double* w = M.fgrad + 6 * (size_t)f + 3 * M.cone_side[i];
-            G wd[DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(w + d));
-            double un[D::NC], an[D::NA];
-            if (NS > 0 && P.eos == ABL_EOS_NASA7) {
-                cell_aux<DIM, NS>(P, un, aux, n, an);
-            } else {
-                load_state<DIM, NS>(U, n, un);
-                cell_aux<DIM, NS>(P, un, aux, n, an);
-            }
-#pragma unroll
-            for (int k = 0; k < D::NA; k++) {
-                const G delta = G(an[k] - ac[k]);
-#pragma unroll
-                for (int d = 0; d < DIM; d++) ga[k * DIM + d] += wd[d] * delta;
-            }
-        }
-        G* out = agrad + (size_t)c * D::NA * DIM;
+    if (do_aux) {
+        G* out = agrad + (size_t)c * GR::AS;
 #pragma unroll
         for (int k = 0; k < D::NA * DIM; k++) out[k] = ga[k];
     }
@@ -299,48 +395,44 @@ __device__ __forceinline__ void advection_split(const Phys& P, const double* nor
 
 // ---------------------------------------------------------------------------------------------------
 // flux of one face: advection (NS + species) and diffusion (NS + species), summed per component
-template <int DIM, int NS, class G>
+template <int DIM, int NS, class G, int FK>
 __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L, int R, const double* normal, const double* fdx,
-                                          const double* __restrict__ U, const double* __restrict__ aux, const G* __restrict__ grad,
-                                          const G* __restrict__ agrad, double* flux, bool* ok, bool* rok) {
+                                          const double* __restrict__ U, const double* __restrict__ dU, const double* __restrict__ aux,
+                                          const G* __restrict__ grad, const G* __restrict__ agrad, StateOf<G>* flux, bool* ok, bool* rok) {
     using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, G>;
+    using S = StateOf<G>;
 #pragma unroll
     for (int k = 0; k < D::NC; k++) flux[k] = 0.0;
-    double cL[D::NC], cR[D::NC];
-    load_state<DIM, NS>(U, L, cL);
-    load_state<DIM, NS>(U, R, cR);
+    S cL[D::NC], cR[D::NC];
+    load_state<DIM, NS, S>(U, dU, L, cL);
+    load_state<DIM, NS, S>(U, dU, R, cR);
     const bool adv = P.advection && P.flux != ABL_FLUX_OFF;
     const bool spadv = NS > 0 && P.sp_adv && P.flux != ABL_FLUX_OFF;
     if (adv || spadv) {
         const bool lsq = P.recon == ABL_RECON_LEASTSQUARES;
         // ProjectToFace (cellInterpolant.cpp:890-950): cells with a gradient are projected to the face
-        double uL[D::NC], uR[D::NC];
+        S uL[D::NC], uR[D::NC];
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
             uL[k] = cL[k];
             uR[k] = cR[k];
         }
         if (lsq) {
-            const uint8_t kL = M.kind[L], kR = M.kind[R];
-            if (kL == ABL_CELL_OWNED || kL == ABL_CELL_HALO) {
-                const G* g = grad + (size_t)L * D::NC * DIM;
+            // cells without a gradient hold a zero row, so u + 0 . dx = u exactly
+            G gL[D::NC * DIM], gR[D::NC * DIM];
+            load_row<D::NC * DIM, G>(grad + (size_t)L * GR::GS, gL);
+            load_row<D::NC * DIM, G>(grad + (size_t)R * GR::GS, gR);
 #pragma unroll
-                for (int k = 0; k < D::NC; k++) {
-                    G dot = 0;
+            for (int k = 0; k < D::NC; k++) {
+                G dotL = 0, dotR = 0;
 #pragma unroll
-                    for (int d = 0; d < DIM; d++) dot += __ldg(g + k * DIM + d) * G(fdx[d]);
-                    uL[k] = uL[k] + double(dot);
+                for (int d = 0; d < DIM; d++) {
+                    dotL += gL[k * DIM + d] * G(fdx[d]);
+                    dotR += gR[k * DIM + d] * G(fdx[3 + d]);
                 }
-            }
-            if (kR == ABL_CELL_OWNED || kR == ABL_CELL_HALO) {
-                const G* g = grad + (size_t)R * D::NC * DIM;
-#pragma unroll
-                for (int k = 0; k < D::NC; k++) {
-                    G dot = 0;
-#pragma unroll
-                    for (int d = 0; d < DIM; d++) dot += __ldg(g + k * DIM + d) * G(fdx[3 + d]);
-                    uR[k] = uR[k] + double(dot);
-                }
+                uL[k] = uL[k] + to_state<S>(dotL);
+                uR[k] = uR[k] + to_state<S>(dotR);
             }
         }
         double TL = 300.0, TR = 300.0;
@@ -348,9 +440,14 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
             TL = __ldg(aux + (size_t)L * D::NA);
             TR = __ldg(aux + (size_t)R * D::NA);
         }
-        if (std::is_same<G, float>::value && (P.flux == ABL_FLUX_AUSM || P.flux == ABL_FLUX_AUSMPUP)) {
-            advection_split<DIM, NS>(P, normal, uL, uR, TL, TR, adv, spadv, flux, ok);
-        } else {
+        bool split = false;
+        if constexpr (std::is_same<G, float>::value) {
+            if (FK == ABL_FLUX_AUSM || FK == ABL_FLUX_AUSMPUP || (FK < 0 && (P.flux == ABL_FLUX_AUSM || P.flux == ABL_FLUX_AUSMPUP))) {
+                advection_split<DIM, NS>(P, normal, uL, uR, TL, TR, adv, spadv, flux, ok);
+                split = true;
+            }
+        }
+        if (!split) {
             // NavierStokesTransport::AdvectionFlux (navierStokesTransport.cpp:99-207)
             double areaMag = 0;
 #pragma unroll
@@ -360,11 +457,11 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
             double norm[DIM];
 #pragma unroll
             for (int d = 0; d < DIM; d++) norm[d] = normal[d] * iA;
-            const Decoded dL = decode<DIM, NS>(P, NS, uL, TL * .67 + .33 * TR, ok);
-            const Decoded dR = decode<DIM, NS>(P, NS, uR, TL * .33 + .67 * TR, ok);
-            const double rhoL = uL[0], rhoR = uR[0];
-            const double irhoL = rcp64(rhoL), irhoR = rcp64(rhoR);
-            double velL[DIM], velR[DIM], unL = 0, unR = 0;
+            const auto dL = decode<DIM, NS>(P, NS, uL, TL * .67 + .33 * TR, ok);
+            const auto dR = decode<DIM, NS>(P, NS, uR, TL * .33 + .67 * TR, ok);
+            const S rhoL = uL[0], rhoR = uR[0];
+            const S irhoL = rcp64(rhoL), irhoR = rcp64(rhoR);
+            S velL[DIM], velR[DIM], unL = 0, unR = 0;
 #pragma unroll
             for (int d = 0; d < DIM; d++) {
                 velL[d] = uL[2 + d] * irhoL;
@@ -372,38 +469,38 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
                 velR[d] = uR[2 + d] * irhoR;
                 unR += velR[d] * norm[d];
             }
-            double mf, p12;
-            const int dir = flux_calc<double>(P, unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p, &mf, &p12, rok);
+            S mf, p12;
+            const int dir = flux_calc_k<FK, S>(P, unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p, &mf, &p12, rok);
             if (adv) {
                 flux[0] = mf * areaMag;
                 if (dir == ABL_DIR_LEFT) {
-                    double v2 = 0;
+                    S v2 = 0;
 #pragma unroll
                     for (int d = 0; d < DIM; d++) v2 += velL[d] * velL[d];
-                    const double velMag = sqrt(v2);
-                    const double H = dL.e + velMag * velMag / 2.0 + dL.p * irhoL;
+                    const S velMag = dsqrt(v2);
+                    const S H = dL.e + velMag * velMag / 2.0 + dL.p * irhoL;
                     flux[1] = H * mf * areaMag;
 #pragma unroll
                     for (int n = 0; n < DIM; n++) flux[2 + n] = velL[n] * mf * areaMag + p12 * normal[n];
                 } else if (dir == ABL_DIR_RIGHT) {
-                    double v2 = 0;
+                    S v2 = 0;
 #pragma unroll
                     for (int d = 0; d < DIM; d++) v2 += velR[d] * velR[d];
-                    const double velMag = sqrt(v2);
-                    const double H = dR.e + velMag * velMag / 2.0 + dR.p * irhoR;
+                    const S velMag = dsqrt(v2);
+                    const S H = dR.e + velMag * velMag / 2.0 + dR.p * irhoR;
                     flux[1] = H * mf * areaMag;
 #pragma unroll
                     for (int n = 0; n < DIM; n++) flux[2 + n] = velR[n] * mf * areaMag + p12 * normal[n];
                 } else {
-                    double v2L = 0, v2R = 0;
+                    S v2L = 0, v2R = 0;
 #pragma unroll
                     for (int d = 0; d < DIM; d++) {
                         v2L += velL[d] * velL[d];
                         v2R += velR[d] * velR[d];
                     }
-                    const double mL = sqrt(v2L), mR = sqrt(v2R);
-                    const double HL = dL.e + mL * mL / 2.0 + dL.p * irhoL;
-                    const double HR = dR.e + mR * mR / 2.0 + dR.p * irhoR;
+                    const S mL = dsqrt(v2L), mR = dsqrt(v2R);
+                    const S HL = dL.e + mL * mL / 2.0 + dL.p * irhoL;
+                    const S HR = dR.e + mR * mR / 2.0 + dR.p * irhoR;
                     flux[1] = 0.5 * (HL + HR) * mf * areaMag;
 #pragma unroll
                     for (int n = 0; n < DIM; n++) flux[2 + n] = 0.5 * (velL[n] + velR[n]) * mf * areaMag + p12 * normal[n];
@@ -426,27 +523,28 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
     if (dif || spdif) {
         // FaceInterpolant: face value = average of the two cells, face gradient = average of the two
         // cells' least-squares gradients (LeastSquaresAverage with numberStencils = 2)
-        double fs[D::NC], fa[D::NA], aL[D::NA], aR[D::NA];
+        S fs[D::NC], fa[D::NA], aL[D::NA], aR[D::NA];
         cell_aux<DIM, NS>(P, cL, aux, L, aL);
         cell_aux<DIM, NS>(P, cR, aux, R, aR);
 #pragma unroll
         for (int k = 0; k < D::NC; k++) fs[k] = cL[k] * 0.5 + cR[k] * 0.5;
 #pragma unroll
         for (int k = 0; k < D::NA; k++) fa[k] = aL[k] * 0.5 + aR[k] * 0.5;
-        const G* gL = agrad + (size_t)L * D::NA * DIM;
-        const G* gR = agrad + (size_t)R * D::NA * DIM;
-        double mu, kc, diff;
+        G gL[D::NA * DIM], gR[D::NA * DIM];
+        load_row<D::NA * DIM, G>(agrad + (size_t)L * GR::AS, gL);
+        load_row<D::NA * DIM, G>(agrad + (size_t)R * GR::AS, gR);
+        S mu, kc, diff;
         transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
         if (dif) {
             // NavierStokesTransport::DiffusionFlux + CompressibleFlowComputeStressTensor (navierStokesTransport.cpp:454-532)
             G gv[DIM * DIM];
 #pragma unroll
-            for (int i = 0; i < DIM * DIM; i++) gv[i] = G(0.5) * __ldg(gL + DIM + i) + G(0.5) * __ldg(gR + DIM + i);
+            for (int i = 0; i < DIM * DIM; i++) gv[i] = G(0.5) * gL[DIM + i] + G(0.5) * gR[DIM + i];
             G divVel = 0;
 #pragma unroll
             for (int c = 0; c < DIM; ++c) divVel += gv[c * DIM + c];
             G tau[DIM * DIM];
-            const G gmu = G(mu);
+            const G gmu = static_cast<G>(mu);
 #pragma unroll
             for (int c = 0; c < DIM; ++c)
 #pragma unroll
@@ -457,25 +555,25 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
                 G vf = 0;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) vf += -G(normal[d]) * tau[c * DIM + d];
-                flux[2 + c] += double(vf);
+                flux[2 + c] += to_state<S>(vf);
             }
             G ef = 0;
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 G heat = 0;
 #pragma unroll
-                for (int c = 0; c < DIM; ++c) heat += G(fa[1 + c]) * tau[d * DIM + c];
-                heat += G(kc) * (G(0.5) * __ldg(gL + d) + G(0.5) * __ldg(gR + d));
+                for (int c = 0; c < DIM; ++c) heat += static_cast<G>(fa[1 + c]) * tau[d * DIM + c];
+                heat += static_cast<G>(kc) * (G(0.5) * gL[d] + G(0.5) * gR[d]);
                 heat *= -G(normal[d]);
                 ef += heat;
             }
-            flux[1] += double(ef);
+            flux[1] += to_state<S>(ef);
         }
         if constexpr (NS > 0) {
             if (spdif) {
                 // SpeciesTransport::DiffusionEnergyFlux + DiffusionSpeciesFlux (speciesTransport.cpp:112-228)
-                const double density = fs[0];
-                double hs[NS];
+                const S density = fs[0];
+                S hs[NS];
                 if (P.eos == ABL_EOS_NASA7) {
 #pragma unroll
                     for (int s = 0; s < NS; s++) hs[s] = nasa_h_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s] - P.href[s];
@@ -484,13 +582,13 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
                     for (int s = 0; s < NS; s++) hs[s] = 0.0;
                 }
                 const int yoff = (1 + DIM) * DIM;
-                double ef = 0;
+                S ef = 0;
 #pragma unroll
                 for (int s = 0; s < NS; ++s) {
-                    double sf = 0;
+                    S sf = 0;
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) {
-                        const double gy = double(G(0.5) * __ldg(gL + yoff + s * DIM + d) + G(0.5) * __ldg(gR + yoff + s * DIM + d));
+                        const S gy = to_state<S>(G(0.5) * gL[yoff + s * DIM + d] + G(0.5) * gR[yoff + s * DIM + d]);
                         ef += -normal[d] * density * diff * hs[s] * gy;
                         sf += -normal[d] * density * diff * gy;
                     }
@@ -505,12 +603,16 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 // ---------------------------------------------------------------------------------------------------
 // One CTA per tile. Phase 1: face fluxes into shared memory (tile-ordered geometry streamed from HBM).
 // Phase 2: each tile cell adds -+flux/V of its faces in ascending face order and writes F once.
-template <int DIM, int NS, class G>
-__global__ void __launch_bounds__(128, (NS > 2 ? 2 : 3)) k_tile_flux(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
-                                                   const G* __restrict__ grad, const G* __restrict__ agrad, double* __restrict__ F,
-                                                   int overwrite, int* status) {
+template <int DIM, int NS, class G, int FK>
+__global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMesh M, Phys P, const double* __restrict__ U,
+                                                                     const double* __restrict__ dU, const double* __restrict__ aux,
+                                                                     const G* __restrict__ grad, const G* __restrict__ agrad,
+                                                                     double* __restrict__ F, double* __restrict__ dF, int overwrite,
+                                                                     int* status) {
     using D = Dims<DIM, NS>;
-    extern __shared__ double sflux[];  // [faces of this tile][NC]
+    using S = StateOf<G>;
+    extern __shared__ double sflux_raw[];
+    S* sflux = reinterpret_cast<S*>(sflux_raw);  // [faces of this tile][NC]
     const int t = blockIdx.x;
     const int fb = M.tile_face_ptr[t], fe = M.tile_face_ptr[t + 1];
     bool ok = true, rok = true;
@@ -524,9 +626,9 @@ __global__ void __launch_bounds__(128, (NS > 2 ? 2 : 3)) k_tile_flux(DevMesh M, 
             fdx[d] = __ldg(M.tf_fdx + 6 * (size_t)i + d);
             fdx[3 + d] = __ldg(M.tf_fdx + 6 * (size_t)i + 3 + d);
         }
-        double flux[D::NC];
-        face_flux<DIM, NS, G>(M, P, lr.x, lr.y, normal, fdx, U, aux, grad, agrad, flux, &ok, &rok);
-        double* out = sflux + (size_t)(i - fb) * D::NC;
+        S flux[D::NC];
+        face_flux<DIM, NS, G, FK>(M, P, lr.x, lr.y, normal, fdx, U, dU, aux, grad, agrad, flux, &ok, &rok);
+        S* out = sflux + (size_t)(i - fb) * D::NC;
 #pragma unroll
         for (int k = 0; k < D::NC; k++) out[k] = flux[k];
     }
@@ -536,18 +638,23 @@ __global__ void __launch_bounds__(128, (NS > 2 ? 2 : 3)) k_tile_flux(DevMesh M, 
     for (int j = cb + threadIdx.x; j < ce; j += blockDim.x) {
         const int c = M.tile_cells[j];
         const double iv = M.ivol[c];
-        double acc[D::NC];
+        S acc[D::NC];
         if (overwrite) {
 #pragma unroll
             for (int k = 0; k < D::NC; k++) acc[k] = 0.0;
         } else {
 #pragma unroll
-            for (int k = 0; k < D::NC; k++) acc[k] = F[(size_t)c * D::NC + k];
+            for (int k = 0; k < D::NC; k++) {
+                if constexpr (std::is_same<S, Dual>::value)
+                    acc[k] = Dual(F ? F[(size_t)c * D::NC + k] : 0.0, dF[(size_t)c * D::NC + k]);
+                else
+                    acc[k] = F[(size_t)c * D::NC + k];
+            }
         }
         const int e0 = M.tc_fptr[j], e1 = M.tc_fptr[j + 1];
         for (int e = e0; e < e1; e++) {
             const uint16_t code = M.tc_face[e];
-            const double* ff = sflux + (size_t)(code & 0x7fff) * D::NC;
+            const S* ff = sflux + (size_t)(code & 0x7fff) * D::NC;
             if (code & 0x8000) {
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) acc[k] += ff[k] * iv;
@@ -558,8 +665,13 @@ __global__ void __launch_bounds__(128, (NS > 2 ? 2 : 3)) k_tile_flux(DevMesh M, 
         }
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
-            F[(size_t)c * D::NC + k] = acc[k];
-            finite = finite && isfinite(acc[k]);
+            if constexpr (std::is_same<S, Dual>::value) {
+                if (F) F[(size_t)c * D::NC + k] = acc[k].v;
+                dF[(size_t)c * D::NC + k] = acc[k].d;
+            } else {
+                F[(size_t)c * D::NC + k] = acc[k];
+            }
+            finite = finite && dfinite(acc[k]);
         }
     }
     if (!finite) atomicOr(status, kStatusNaN);

@@ -1,0 +1,92 @@
+// fv_launch.cuh -- the launch sequences of one RHS / aux update / tangent evaluation for a compiled
+// (DIM, NS) instance. Included only by the fv_inst_*.cu translation units, which instantiate them.
+#pragma once
+#include "fv_handle.hpp"
+
+namespace abl {
+
+template <int DIM, int NS, class G, int FK>
+void launch_tile(abl_fv* fv, const double* U, const double* dU, const G* grad, const G* agrad, double* F, double* dF, int overwrite,
+                 cudaStream_t s) {
+    auto kern = k_tile_flux<DIM, NS, G, FK>;
+    const int smem = fv->tile_smem * (std::is_same<G, Dual>::value ? 2 : 1);
+    if (smem > 227 * 1024) throw AblError(ABL_ERR_UNSUPPORTED, "tile flux buffer exceeds shared memory for this species count");
+    ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<fv->mesh.n_tiles, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p);
+    check_launch();
+}
+
+template <int DIM, int NS, class G, int LIM>
+void launch_gradient(abl_fv* fv, const double* U, const double* dU, G* grad, G* agrad, cudaStream_t s) {
+    k_gradient<DIM, NS, G, LIM><<<blocks_for(fv->mesh.n_cells, 128), 128, 0, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad,
+                                                                                  fv->need_state_grad, fv->need_aux_grad);
+    check_launch();
+}
+
+// the RHS for gradient storage type G: limiter and flux calculator fixed at compile time where a
+// specialised kernel exists (minmod; AUSM, AUSM+up), chosen at run time otherwise
+template <int DIM, int NS, class G>
+void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int overwrite, cudaStream_t s) {
+    const Phys& P = fv->phys;
+    if (fv->need_state_grad || fv->need_aux_grad) {
+        mark(fv, "k_gradient", s);
+        if (P.limiter == ABL_LIMITER_MINMOD)
+            launch_gradient<DIM, NS, G, ABL_LIMITER_MINMOD>(fv, U, nullptr, grad, agrad, s);
+        else
+            launch_gradient<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, s);
+    }
+    mark(fv, "k_tile_flux", s);
+    if (fv->mesh.n_tiles > 0) {
+        if (P.flux == ABL_FLUX_AUSMPUP)
+            launch_tile<DIM, NS, G, ABL_FLUX_AUSMPUP>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
+        else if (P.flux == ABL_FLUX_AUSM)
+            launch_tile<DIM, NS, G, ABL_FLUX_AUSM>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
+        else
+            launch_tile<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
+    }
+}
+
+template <int DIM, int NS>
+void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
+    const DevMesh& M = fv->mesh;
+    fv->n_marks = 0;
+    if (fv->need_aux) {
+        mark(fv, "k_aux", s);
+        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, fv->phys, U, fv->aux.p, fv->status.p);
+        check_launch();
+    }
+    if (precision == ABL_PRECISION_MIXED)
+        rhs_with<DIM, NS, float>(fv, U, fv->grad32.p, fv->agrad32.p, F, overwrite, s);
+    else
+        rhs_with<DIM, NS, double>(fv, U, fv->grad64.p, fv->agrad64.p, F, overwrite, s);
+    mark(fv, "end", s);
+}
+
+template <int DIM, int NS>
+void run_aux(abl_fv* fv, const double* U, cudaStream_t s) {
+    k_aux<DIM, NS><<<blocks_for(fv->mesh.n_cells, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->aux.p, fv->status.p);
+    check_launch();
+}
+
+// forward tangent: the FP64 RHS kernels evaluated on Dual numbers (value + one directional derivative)
+template <int DIM, int NS>
+void run_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* dF, cudaStream_t s) {
+    const DevMesh& M = fv->mesh;
+    fv->n_marks = 0;
+    if (fv->need_aux) {
+        mark(fv, "k_aux", s);
+        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, fv->phys, U, fv->aux.p, fv->status.p);
+        check_launch();
+    }
+    Dual* grad = reinterpret_cast<Dual*>(fv->gradD.p);
+    Dual* agrad = reinterpret_cast<Dual*>(fv->agradD.p);
+    if (fv->need_state_grad || fv->need_aux_grad) {
+        mark(fv, "k_gradient_tangent", s);
+        launch_gradient<DIM, NS, Dual, -1>(fv, U, dU, grad, agrad, s);
+    }
+    mark(fv, "k_tile_flux_tangent", s);
+    if (M.n_tiles > 0) launch_tile<DIM, NS, Dual, -1>(fv, U, dU, grad, agrad, F, dF, 0, s);
+    mark(fv, "end", s);
+}
+
+}  // namespace abl

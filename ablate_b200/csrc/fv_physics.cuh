@@ -17,6 +17,8 @@
 #include <stdint.h>
 
 #include "../../include/ablate_fv.h"
+#include "fv_dual.cuh"
+#include <type_traits>
 
 namespace abl {
 
@@ -53,6 +55,9 @@ ABL_HD double dabs(double x) { return fabs(x); }
 ABL_HD float dabs(float x) { return fabsf(x); }
 ABL_HD double dpow(double a, double b) { return pow(a, b); }
 ABL_HD float dpow(float a, float b) { return powf(a, b); }
+ABL_HD double dsin(double x) { return sin(x); }
+ABL_HD float dsin(float x) { return sinf(x); }
+ABL_HD bool dfinite(double x) { return isfinite(x); }
 
 // Physics parameters resident on the device (passed by value to kernels).
 struct Phys {
@@ -281,6 +286,10 @@ ABL_HD int flux_riemann(R gamma, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R
     return uX > R(0) ? ABL_DIR_LEFT : ABL_DIR_RIGHT;
 }
 
+// Flux calculator fixed at compile time (FK >= 0) or chosen at run time from P.flux (FK < 0).
+template <int FK, class R>
+ABL_HD int flux_calc_k(const Phys& P, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R pR, R* mf, R* p12, bool* ok);
+
 template <class R>
 ABL_HD int flux_calc(const Phys& P, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R pR, R* mf, R* p12, bool* ok) {
     switch (P.flux) {
@@ -300,6 +309,17 @@ ABL_HD int flux_calc(const Phys& P, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR
             return ABL_DIR_NA;
     }
 }
+
+template <int FK, class R>
+ABL_HD int flux_calc_k(const Phys& P, R uL, R aL, R rhoL, R pL, R uR, R aR, R rhoR, R pR, R* mf, R* p12, bool* ok) {
+    if constexpr (FK == ABL_FLUX_AUSM) return flux_ausm<R>(uL, aL, rhoL, pL, uR, aR, rhoR, pR, mf, p12);
+    if constexpr (FK == ABL_FLUX_AUSMPUP) return flux_ausmpup<R>(R(P.minf), R(P.alpha), uL, aL, rhoL, pL, uR, aR, rhoR, pR, mf, p12);
+    return flux_calc<R>(P, uL, aL, rhoL, pL, uR, aR, rhoR, pR, mf, p12, ok);
+}
+
+// Limiter fixed at compile time (LIM >= 0) or chosen at run time (LIM < 0).
+template <int LIM, class R>
+ABL_HD R limiter_k(int kind, R f);
 
 // ------------------------------------------------------------------------------------------------
 // Split form of the AUSM-family fluxes for the mixed-precision path.
@@ -422,27 +442,31 @@ ABL_HD SplitFlux flux_split(const Phys& P, double rhoL, double pL, double unAL, 
 
 // ------------------------------------------------------------------------------------------------
 // NASA-7 mixture thermodynamics (always FP64: the secant temperature solve and the energies it
-// differences need the full mantissa)
+// differences need the full mantissa). Templated on the state scalar S (double, or Dual for the
+// tangent kernels).
 // ------------------------------------------------------------------------------------------------
 // molar enthalpy (J/kmol) of species k: R T (a1 + a2 T/2 + a3 T^2/3 + a4 T^3/4 + a5 T^4/5 + a6/T)
-ABL_HD double nasa_h_molar(const double* c, double T) {
+template <class S>
+ABL_HD S nasa_h_molar(const double* c, S T) {
     const double* a = (T < c[0]) ? c + 1 : c + 8;
     return kRuniv * T * (a[0] + T * (a[1] * 0.5 + T * (a[2] * (1.0 / 3.0) + T * (a[3] * 0.25 + T * a[4] * 0.2))) + a[5] / T);
 }
-ABL_HD double nasa_cp_molar(const double* c, double T) {
+template <class S>
+ABL_HD S nasa_cp_molar(const double* c, S T) {
     const double* a = (T < c[0]) ? c + 1 : c + 8;
     return kRuniv * (a[0] + T * (a[1] + T * (a[2] + T * (a[3] + T * a[4]))));
 }
 
 // Y from densityYi with the reference's clipping (TChem::FillWorkingVectorFromDensityMassFractions,
 // src/eos/tChem.cpp:581-602); ns may be a compile-time constant after inlining.
-ABL_HD void fill_y(int ns, double rho, const double* rhoY, double* ys) {
-    double sum = 0.0;
-    const double irho = rcp64(rho);
+template <class S>
+ABL_HD void fill_y(int ns, S rho, const S* rhoY, S* ys) {
+    S sum = 0.0;
+    const S irho = rcp64(rho);
 #pragma unroll
     for (int s = 0; s < ns - 1; s++) {
-        double y = pmax(0.0, rhoY[s] * irho);
-        y = pmin(1.0, y);
+        S y = pmax(S(0.0), rhoY[s] * irho);
+        y = pmin(S(1.0), y);
         ys[s] = y;
         sum += y;
     }
@@ -457,8 +481,9 @@ ABL_HD void fill_y(int ns, double rho, const double* rhoY, double* ys) {
 
 // SensibleInternalEnergyFcn (src/eos/tChem/sensibleInternalEnergyFcn.hpp:25-44):
 // e_s = sum_k Y_k (h_k(T)/W_k - h_ref,k - Ru T / W_k)
-ABL_HD double e_sens(const Phys& P, int ns, const double* ys, double T) {
-    double e = 0;
+template <class S, class ST>
+ABL_HD S e_sens(const Phys& P, int ns, const S* ys, ST T) {
+    S e = 0;
 #pragma unroll
     for (int k = 0; k < ns; k++) e += (nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k]) * ys[k];
     return e;
@@ -501,29 +526,50 @@ ABL_HD double nasa_temperature(const Phys& P, int ns, const double* ys, double e
     return t2;
 }
 
-ABL_HD double mixture_cp(const Phys& P, int ns, const double* ys, double T) {
-    double cp = 0;
+template <class S>
+ABL_HD S mixture_cp(const Phys& P, int ns, const S* ys, S T) {
+    S cp = 0;
 #pragma unroll
     for (int k = 0; k < ns; k++) cp += ys[k] * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
     return cp;
 }
-ABL_HD double mixture_mw(const Phys& P, int ns, const double* ys) {
-    double iw = 0;
+template <class S>
+ABL_HD S mixture_mw(const Phys& P, int ns, const S* ys) {
+    S iw = 0;
 #pragma unroll
     for (int k = 0; k < ns; k++) iw += ys[k] * P.inv_mw[k];
-    return 1.0 / iw;
+    return rcp64(iw);
+}
+
+// Mixture temperature for a state scalar S: the secant iteration on the values; for a Dual state the
+// derivative follows from e_s(T, Y) = e_ref by the implicit-function theorem,
+//   dT = (de_ref - sum_k de_s/dY_k dY_k) / (de_s/dT),  de_s/dT = sum_k Y_k (cp_k - Ru) / W_k = cv
+template <int NSMAX, class S>
+ABL_HD S nasa_temperature_s(const Phys& P, int ns, const S* ys, S eRef, double Tguess, bool* ok) {
+    if constexpr (std::is_same<S, double>::value) {
+        return nasa_temperature(P, ns, ys, eRef, Tguess, ok);
+    } else {
+        double yv[NSMAX > 0 ? NSMAX : 1];
+        for (int k = 0; k < ns; k++) yv[k] = ys[k].v;
+        const double T = nasa_temperature(P, ns, yv, eRef.v, Tguess, ok);
+        const S res = e_sens(P, ns, ys, T) - eRef;  // derivative part: sum de_s/dY dY - de_ref
+        double cv = 0;
+        for (int k = 0; k < ns; k++) cv += yv[k] * (nasa_cp_molar(P.nasa7 + 15 * k, T) - kRuniv) * P.inv_mw[k];
+        return S(T, -res.d / cv);
+    }
 }
 
 // Decoded thermodynamic state of one face side (what AdvectionFlux pulls out of the EOS).
+template <class S>
 struct Decoded {
-    double T, e, a, p;
+    S T, e, a, p;
 };
 
 // Internal energy recovery e = E/rho - |u|^2/2 (always FP64).
-template <int DIM>
-ABL_HD double internal_energy(const double* U) {
-    const double irho = rcp64(U[0]);
-    double ke = 0.0;
+template <int DIM, class S>
+ABL_HD S internal_energy(const S* U) {
+    const S irho = rcp64(U[0]);
+    S ke = 0.0;
 #pragma unroll
     for (int i = 0; i < DIM; i++) ke += sqr(U[2 + i] * irho);
     return U[1] * irho - 0.5 * ke;
@@ -533,53 +579,53 @@ ABL_HD double internal_energy(const double* U) {
 //   PerfectGas: T = e/cv, e(T) = cv T, a(T) = sqrt(gamma R rho T / rho), p(T) = R rho T
 //   NASA-7:     T by secant, e_s(T), a = sqrt(gamma R T) with gamma = cp/(cp - R), p = rho Ru T / W
 // NSMAX sizes the mass-fraction scratch; ns is the species count.
-template <int DIM, int NSMAX>
-ABL_HD Decoded decode(const Phys& P, int ns, const double* U, double Tguess, bool* ok) {
-    Decoded d;
-    const double rho = U[0];
+template <int DIM, int NSMAX, class S>
+ABL_HD Decoded<S> decode(const Phys& P, int ns, const S* U, double Tguess, bool* ok) {
+    Decoded<S> d;
+    const S rho = U[0];
     if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) {
         // T = e/cv, e(T) = cv T, p(T) = R rho T, a(T) = sqrt(gamma p / rho) = sqrt(gamma R T)
-        const double e = internal_energy<DIM>(U);
+        const S e = internal_energy<DIM>(U);
         const double cv = P.r_gas / (P.gamma - 1.0);
         d.T = e * rcp64(cv);
         d.e = d.T * cv;
         d.p = P.r_gas * rho * d.T;
-        d.a = sqrt(P.gamma * P.r_gas * d.T);
+        d.a = dsqrt(P.gamma * P.r_gas * d.T);
         return d;
     }
-    double ys[NSMAX > 0 ? NSMAX : 1];
+    S ys[NSMAX > 0 ? NSMAX : 1];
     fill_y(ns, rho, U + 2 + DIM, ys);
-    const double eRef = internal_energy<DIM>(U);
-    d.T = nasa_temperature(P, ns, ys, eRef, Tguess, ok);
+    const S eRef = internal_energy<DIM>(U);
+    d.T = nasa_temperature_s<NSMAX>(P, ns, ys, eRef, Tguess, ok);
     d.e = e_sens(P, ns, ys, d.T);
-    const double cp = mixture_cp(P, ns, ys, d.T);
-    const double mwMix = mixture_mw(P, ns, ys);
-    const double R = kRuniv / mwMix;
-    const double cv = cp - R;
-    const double gamma = cp * rcp64(cv);
-    d.a = sqrt(gamma * R * d.T);
+    const S cp = mixture_cp(P, ns, ys, d.T);
+    const S mwMix = mixture_mw(P, ns, ys);
+    const S R = kRuniv * rcp64(mwMix);
+    const S cv = cp - R;
+    const S gamma = cp * rcp64(cv);
+    d.a = dsqrt(gamma * R * d.T);
     d.p = rho * R * d.T;
     return d;
 }
 
 // Temperature only (aux update)
-template <int DIM, int NSMAX>
-ABL_HD double temperature(const Phys& P, int ns, const double* U, double Tguess, bool* ok) {
+template <int DIM, int NSMAX, class S>
+ABL_HD S temperature(const Phys& P, int ns, const S* U, double Tguess, bool* ok) {
     if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) {
-        const double e = internal_energy<DIM>(U);
+        const S e = internal_energy<DIM>(U);
         return e * rcp64(P.r_gas / (P.gamma - 1.0));
     }
-    double ys[NSMAX > 0 ? NSMAX : 1];
+    S ys[NSMAX > 0 ? NSMAX : 1];
     fill_y(ns, U[0], U + 2 + DIM, ys);
-    const double eRef = internal_energy<DIM>(U);
-    return nasa_temperature(P, ns, ys, eRef, Tguess, ok);
+    const S eRef = internal_energy<DIM>(U);
+    return nasa_temperature_s<NSMAX>(P, ns, ys, eRef, Tguess, ok);
 }
 
 // cp at temperature T (Sutherland / constant-Lewis conductivity)
-template <int DIM, int NSMAX>
-ABL_HD double cp_at(const Phys& P, int ns, const double* U, double T) {
-    if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) return P.gamma * P.r_gas / (P.gamma - 1.0);
-    double ys[NSMAX > 0 ? NSMAX : 1];
+template <int DIM, int NSMAX, class S>
+ABL_HD S cp_at(const Phys& P, int ns, const S* U, S T) {
+    if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) return S(P.gamma * P.r_gas / (P.gamma - 1.0));
+    S ys[NSMAX > 0 ? NSMAX : 1];
     fill_y(ns, U[0], U + 2 + DIM, ys);
     return mixture_cp(P, ns, ys, T);
 }
@@ -587,13 +633,14 @@ ABL_HD double cp_at(const Phys& P, int ns, const double* U, double T) {
 // ------------------------------------------------------------------------------------------------
 // transport
 // ------------------------------------------------------------------------------------------------
-ABL_HD double sutherland_mu(double T) {
+template <class S>
+ABL_HD S sutherland_mu(S T) {
     const double muo = 1.716e-5, to = 273.e+0, so = 111.e+0;
-    return muo * sqrt(T / to) * (T / to) * (to + so) / (T + so);
+    return muo * dsqrt(T / to) * (T / to) * (to + so) / (T + so);
 }
 
-template <int DIM, int NSMAX>
-ABL_HD void transport(const Phys& P, int ns, const double* U, double T, double* mu, double* k, double* diff) {
+template <int DIM, int NSMAX, class S>
+ABL_HD void transport(const Phys& P, int ns, const S* U, S T, S* mu, S* k, S* diff) {
     switch (P.transport) {
         case ABL_TRANSPORT_CONSTANT:
             *mu = P.mu;
@@ -602,14 +649,14 @@ ABL_HD void transport(const Phys& P, int ns, const double* U, double T, double* 
             return;
         case ABL_TRANSPORT_SUTHERLAND: {
             const double pr = 0.707, sc = 0.707;
-            double m = sutherland_mu(T);
+            S m = sutherland_mu(T);
             *mu = m;
             *k = m * cp_at<DIM, NSMAX>(P, ns, U, T) / pr;
             *diff = m / U[0] / sc;
             return;
         }
         case ABL_TRANSPORT_CONSTANT_LEWIS: {
-            double cp = cp_at<DIM, NSMAX>(P, ns, U, T);
+            S cp = cp_at<DIM, NSMAX>(P, ns, U, T);
             *mu = P.mu;
             *k = P.mu * cp / P.k;
             *diff = *k / (U[0] * cp * P.diff);
@@ -638,11 +685,16 @@ ABL_HD R limiter(int kind, R f) {
             return pmax(R(0), R(2) * f * (R(1) - f) / (sqr(f) + sqr(R(1) - f)));
         case ABL_LIMITER_SIN: {
             R fclip = pmax(pmin(f, R(1)), R(0));
-            return sin(R(3.14159265358979323846) * fclip);
+            return dsin(R(3.14159265358979323846) * fclip);
         }
         default:
             return R(1);
     }
+}
+
+template <int LIM, class R>
+ABL_HD R limiter_k(int kind, R f) {
+    return limiter<R>(LIM >= 0 ? LIM : kind, f);
 }
 
 }  // namespace abl

@@ -330,6 +330,19 @@ class FiniteVolumeSolver:
         """F += RHS(U) with device pointers (e.g. torch tensors' data_ptr()), enqueued on `stream`."""
         L.check(L.lib.abl_fv_rhs(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(F_ptr), precision, C.c_void_p(stream)), "abl_fv_rhs")
 
+    def ComputeJVP(self, time: float, locX: np.ndarray, dX: np.ndarray, dF: np.ndarray, F: np.ndarray | None = None):
+        """dF += J(locX) dX (and F += RHS(locX) when F is given), host arrays (n_cells, nc)."""
+        x = np.ascontiguousarray(locX, dtype=np.float64)
+        dx = np.ascontiguousarray(dX, dtype=np.float64)
+        assert dF.dtype == np.float64 and dF.flags.c_contiguous
+        L.check(L.lib.abl_fv_jvp_host(self.handle, time, L.dptr(x), L.dptr(dx), L.dptr(F) if F is not None else None, L.dptr(dF)),
+                "abl_fv_jvp_host")
+        return dF
+
+    def ComputeJVPDevice(self, time: float, U_ptr: int, dU_ptr: int, dF_ptr: int, F_ptr: int = 0, stream: int = 0):
+        L.check(L.lib.abl_fv_jvp(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(dU_ptr), C.c_void_p(F_ptr or None), C.c_void_p(dF_ptr),
+                                 C.c_void_p(stream)), "abl_fv_jvp")
+
     def UpdateAux(self, locX: np.ndarray):
         """Recompute the aux fields (T, u, Y) from host state locX (CellSolver::UpdateAuxFields)."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

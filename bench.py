@@ -271,6 +271,25 @@ def main():
         solver.Profile(False)
         kernels[prec] = {name: ms / args.steps for name, ms in acc.items()}
 
+    # forward tangent (JVP) cost relative to one FP64 RHS, same protocol
+    jvp_ms = None
+    if L.PRECISION_FP64 in results:
+        dU = torch.randn_like(U) * U.abs().mean(0, keepdim=True) * 1e-2
+        dF = torch.zeros_like(U)
+        for _ in range(args.warmup):
+            solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        jev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            jev[k][0].record(stream)
+            solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream)
+            jev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        jvp_ms = sum(a.elapsed_time(b) for a, b in jev) / args.steps
+        if solver.Status() != L.OK:
+            raise RuntimeError("device status after the timed JVP")
+
     # accuracy of the mixed path against FP64 on this workload
     mixed_err = None
     if L.PRECISION_MIXED in results:
@@ -337,6 +356,7 @@ def main():
                        for p, ms in results.items()},
         "mixed_rel_err_vs_fp64": mixed_err,
         "vjp_over_rhs": None,
+        "jvp": {"ms_per_step": jvp_ms, "over_rhs_fp64": (jvp_ms / results[L.PRECISION_FP64]) if jvp_ms else None},
         "e2e": {"value": world * n_cells / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 2 * state_bytes,
                 "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,
                 "path": "abl_fv_rhs_host: pinned host U and F copied in, RHS, F copied out, every step"},

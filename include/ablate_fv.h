@@ -182,6 +182,15 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
 /* Same with host pointers (the plain PETSc Vec case): copies U in, runs abl_fv_rhs, adds into F. */
 int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision);
 
+/* Forward tangent (JVP) of abl_fv_rhs at FP64: dF += J(U) dU for owned cells, and F += RHS(U) when F
+ * is not NULL. The RHS kernels are evaluated on dual numbers (value + one directional derivative), so
+ * every branch (limiter min, flux splittings, upwind choice) is the primal one and its derivative is
+ * that of the active branch; the mixture temperature's derivative comes from the implicit-function
+ * theorem on e_s(T, Y) = e. The reference's counterpart is PETSc's finite-difference Jacobian-vector
+ * product through the same RHS (MatMFFD on TSComputeRHSFunction). */
+int abl_fv_jvp(abl_fv* fv, double time, const double* U_dev, const double* dU_dev, double* F_dev, double* dF_dev, void* stream);
+int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double* dU_host, double* F_host, double* dF_host);
+
 /* Aux fields (T, u, Y). With the NASA-7 mixture EOS every abl_fv_rhs updates them (the resident T is
  * also the next secant guess); with a perfect gas the RHS recomputes them on the fly and they are
  * refreshed only by abl_fv_update_aux. set_aux sets the temperature guess used by the next update. */
