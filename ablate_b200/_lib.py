@@ -73,6 +73,8 @@ SIGNATURES = {
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
     "abl_fv_jvp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_jvp_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp]),
+    "abl_fv_vjp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_vjp_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, _dp]),
     "abl_fv_update_aux": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_update_aux_host": (C.c_int, [C.c_void_p, _dp]),
     "abl_fv_get_aux": (C.c_int, [C.c_void_p, _dp]),

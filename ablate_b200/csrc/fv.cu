@@ -134,6 +134,10 @@ void dispatch_jvp(abl_fv* fv, const double* U, const double* dU, double* F, doub
     ABL_DISPATCH(fv, run_jvp, U, dU, F, dF, s);
 }
 
+void dispatch_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStream_t s) {
+    ABL_DISPATCH(fv, run_vjp, U, Fb, Ub, s);
+}
+
 bool rhs_supported(int dim, int ns) {
     const int key = dim * 100 + ns;
     return key == 100 || key == 200 || key == 202 || key == 300 || key == 302 || key == 305 || key == 309;
@@ -374,6 +378,19 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->tf_fdx.upload(tl.tf_fdx.data(), tl.tf_fdx.size());
         fv->tc_fptr.upload(tl.tc_fptr.data(), tl.tc_fptr.size());
         fv->tc_face.upload(tl.tc_face.data(), tl.tc_face.size());
+        fv->col_base.upload(tl.col_base.data(), tl.col_base.size());
+        fv->col_start.upload(tl.col_start.data(), tl.col_start.size());
+        fv->tf_slot.upload(tl.tf_slot.data(), tl.tf_slot.size());
+        fv->tf_nb.upload(tl.tf_nb.data(), tl.tf_nb.size());
+        fv->face_nb.upload(tl.face_nb.data(), tl.face_nb.size());
+        fv->n_nb = tl.n_nb;
+        for (int k = 0; k < tl.n_tiles; k++) fv->tile_max_cells = std::max(fv->tile_max_cells, tl.cell_ptr[k + 1] - tl.cell_ptr[k]);
+        {
+            std::vector<int32_t> no;
+            for (int c = 0; c < h.n_cells; c++)
+                if (h.kind[c] != ABL_CELL_OWNED) no.push_back(c);
+            fv->nonowned.upload(no.data(), no.size());
+        }
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
 
@@ -416,6 +433,13 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.tf_fdx = fv->tf_fdx.p;
         M.tc_fptr = fv->tc_fptr.p;
         M.tc_face = fv->tc_face.p;
+        M.col_base = fv->col_base.p;
+        M.col_start = fv->col_start.p;
+        M.tf_slot = fv->tf_slot.p;
+        M.tf_nb = fv->tf_nb.p;
+        M.face_nb = fv->face_nb.p;
+        M.n_nonowned = (int)fv->nonowned.n;
+        M.nonowned = fv->nonowned.p;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();
     });
@@ -502,6 +526,43 @@ int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double*
         if (rc != ABL_OK) throw AblError(rc, g_last_error);
         ABL_CUDA(cudaMemcpy(dF_host, fv->hdF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
         if (F_host) ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+int abl_fv_vjp(abl_fv* fv, double time, const double* U_dev, const double* Fbar_dev, double* Ubar_dev, void* stream) {
+    (void)time;
+    return guarded([&] {
+        if (!fv || !U_dev || !Fbar_dev || !Ubar_dev) throw std::invalid_argument("abl_fv_vjp: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        // per-cell adjoint records, allocated on first use
+        const size_t n = (size_t)fv->n_cells;
+        if (fv->adj_ub.n == 0) {
+            if (fv->need_state_grad) fv->adj_gb.alloc(n * round_up(fv->nc * fv->dim, 2));
+            if (fv->need_aux_grad) fv->adj_gab.alloc(n * round_up(fv->naux * fv->dim, 2));
+            fv->adj_beta.alloc(n * fv->nc);
+            fv->adj_fstar.alloc(n * fv->nc);
+            fv->adj_ab.alloc(n * fv->naux);
+            fv->adj_nb.alloc((size_t)std::max(fv->n_nb, 1) * (fv->nc + fv->nc * fv->dim + fv->naux + fv->naux * fv->dim));
+            fv->adj_ub.alloc(n * fv->nc);
+        }
+        dispatch_vjp(fv, U_dev, Fbar_dev, Ubar_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_vjp_host(abl_fv* fv, double time, const double* U_host, const double* Fbar_host, double* Ubar_host) {
+    return guarded([&] {
+        if (!fv || !U_host || !Fbar_host || !Ubar_host) throw std::invalid_argument("abl_fv_vjp_host: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->hU.n != n) fv->hU.alloc(n);
+        if (fv->hdU.n != n) fv->hdU.alloc(n);
+        if (fv->hdF.n != n) fv->hdF.alloc(n);
+        ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        ABL_CUDA(cudaMemcpy(fv->hdF.p, Fbar_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        ABL_CUDA(cudaMemcpy(fv->hdU.p, Ubar_host, n * sizeof(double), cudaMemcpyHostToDevice));
+        int rc = abl_fv_vjp(fv, time, fv->hU.p, fv->hdF.p, fv->hdU.p, nullptr);
+        if (rc != ABL_OK) throw AblError(rc, g_last_error);
+        ABL_CUDA(cudaMemcpy(Ubar_host, fv->hdU.p, n * sizeof(double), cudaMemcpyDeviceToHost));
     });
 }
 

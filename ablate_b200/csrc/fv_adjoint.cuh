@@ -1,0 +1,1089 @@
+// fv_adjoint.cuh -- reverse mode (vector-Jacobian product) of the FP64 RHS, sm_100a.
+//
+// Given a residual weight Fbar (one row per cell, read on owned cells), the VJP accumulates
+// Ubar += (dF/dU)^T Fbar for every cell, boundary ghosts and halos included. It is the exact
+// transpose of the tangent the dual-number kernels propagate (the derivative of the branch the primal
+// evaluation takes at limiter minima, flux-splitting switches and mass-fraction clips).
+//
+// Nothing of the forward pass is stored beyond what one RHS already keeps: the limited gradients and
+// aux gradients from k_gradient. Every other intermediate is recomputed:
+//   k_gradient          forward gradients (the RHS kernel, unchanged)
+//   k_tile_adjoint      one CTA per tile. Per face, colour by colour: recompute the face states, the
+//                       EOS decode and the flux calculator, then run the flux backwards; the adjoint of
+//                       each side's state, limited gradient, aux and aux gradient is summed into that
+//                       cell's shared-memory accumulators (faces of one colour touch distinct cells, so
+//                       no atomics and a fixed order). Then per tile cell: the limiter is recomputed
+//                       (its minimising face per component) and the limiter and least-squares gradient
+//                       are run backwards.
+//   k_adjoint_nonowned  the same cell step for boundary ghosts and halos, from per-face records.
+//   k_adjoint_gather    per cell: the neighbour terms of the gradient, limiter and aux-gradient adjoints
+//                       (a gather over the cell's faces, the transpose of the forward gathers), then the
+//                       aux (T, u, Y) chain rule, added into Ubar.
+//
+// Reference functions reversed: CellInterpolant::ComputeFieldGradients and the limiter
+// (src/finiteVolume/cellInterpolant.cpp:282-497), ComputeFluxSourceTerms and ProjectToFace (:499-639,
+// :890-950), NavierStokesTransport::AdvectionFlux / DiffusionFlux (navierStokesTransport.cpp:99-207,
+// 454-532), SpeciesTransport fluxes (speciesTransport.cpp:112-341), the flux calculators
+// (ausm.cpp:2-43, ausmpUp.cpp:5-96, riemann.cpp / riemannSolver.cpp), PerfectGas and TChem decode.
+#pragma once
+#include "fv_kernels.cuh"
+
+namespace abl {
+
+// ---------------------------------------------------------------------------------------------------
+// EOS pieces
+// ---------------------------------------------------------------------------------------------------
+// e = U1/rho - |rho u|^2 / (2 rho^2)
+template <int DIM>
+ABL_HD void internal_energy_vjp(const double* U, double eb, double* Ub) {
+    const double irho = rcp64(U[0]);
+    double vu = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        const double vel = U[2 + d] * irho;
+        Ub[2 + d] -= eb * vel * irho;
+        vu += vel * U[2 + d];
+    }
+    Ub[1] += eb * irho;
+    Ub[0] -= eb * (U[1] - vu) * irho * irho;
+}
+
+template <class S>
+ABL_HD S nasa_dcp_molar(const double* c, S T) {
+    const double* a = (T < c[0]) ? c + 1 : c + 8;
+    return kRuniv * (a[1] + T * (2.0 * a[2] + T * (3.0 * a[3] + T * 4.0 * a[4])));
+}
+
+// reverse of fill_y (clip to [0, 1], renormalise or close with the last species)
+template <int NSMAX>
+ABL_HD void fill_y_vjp(int ns, double rho, const double* rhoY, const double* ysb, double* rhob, double* rhoYb) {
+    const double irho = rcp64(rho);
+    double y[NSMAX > 0 ? NSMAX : 1];
+    bool act[NSMAX > 0 ? NSMAX : 1];
+    double sum = 0.0;
+#pragma unroll
+    for (int s = 0; s < ns - 1; s++) {
+        const double raw = rhoY[s] * irho;
+        act[s] = raw > 0.0 && !(1.0 < raw);
+        y[s] = pmin(1.0, pmax(0.0, raw));
+        sum += y[s];
+    }
+    double irhob = 0.0, dot = 0.0;
+    if (sum > 1.0) {
+#pragma unroll
+        for (int s = 0; s < ns - 1; s++) dot += ysb[s] * y[s];
+    }
+#pragma unroll
+    for (int s = 0; s < ns - 1; s++) {
+        double yb = sum > 1.0 ? ysb[s] / sum - dot / (sum * sum) : ysb[s] - ysb[ns - 1];
+        if (!act[s]) yb = 0.0;
+        rhoYb[s] += yb * irho;
+        irhob += yb * rhoY[s];
+    }
+    *rhob -= irhob * irho * irho;
+}
+
+// reverse of the mixture temperature T(e_ref, Y) (implicit function of e_s(T, Y) = e_ref)
+template <int DIM, int NSMAX>
+ABL_HD void nasa_temperature_vjp(const Phys& P, int ns, const double* U, const double* ys, double T, double Tb, double* ysb, double* Ub) {
+    double cv = 0;
+#pragma unroll
+    for (int k = 0; k < ns; k++) cv += ys[k] * (nasa_cp_molar(P.nasa7 + 15 * k, T) - kRuniv) * P.inv_mw[k];
+    const double q = Tb / cv;
+#pragma unroll
+    for (int k = 0; k < ns; k++)
+        ysb[k] -= q * (nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k]);
+    internal_energy_vjp<DIM>(U, q, Ub);
+}
+
+// reverse of decode(): adjoints of the decoded e, a, p into the face state U
+template <int DIM, int NSMAX>
+ABL_HD void decode_vjp(const Phys& P, int ns, const double* U, const Decoded<double>& dd, double eb, double ab, double pb, double* Ub) {
+    const double rho = U[0];
+    if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) {
+        const double cv = P.r_gas / (P.gamma - 1.0);
+        double Tb = eb * cv + pb * P.r_gas * rho;
+        if (dd.a > 0) Tb += ab * P.gamma * P.r_gas / (2.0 * dd.a);
+        Ub[0] += pb * P.r_gas * dd.T;
+        internal_energy_vjp<DIM>(U, Tb * rcp64(cv), Ub);
+        return;
+    }
+    constexpr int NY = NSMAX > 0 ? NSMAX : 1;
+    double ys[NY], ysb[NY];
+    fill_y(ns, rho, U + 2 + DIM, ys);
+    const double T = dd.T;
+    double cp = 0, iw = 0, dcp = 0;
+#pragma unroll
+    for (int k = 0; k < ns; k++) {
+        cp += ys[k] * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
+        dcp += ys[k] * nasa_dcp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
+        iw += ys[k] * P.inv_mw[k];
+        ysb[k] = 0.0;
+    }
+    const double R = kRuniv * rcp64(rcp64(iw));
+    const double cv = cp - R;
+    const double gamma = cp * rcp64(cv);
+    const double q = dd.a > 0 ? ab / (2.0 * dd.a) : 0.0;  // a = sqrt(gamma R T)
+    const double gb = q * R * T;
+    double Rb = q * gamma * T + pb * rho * T;
+    double Tb = q * gamma * R + pb * rho * R;
+    Ub[0] += pb * R * T;
+    const double cpb = -gb * R / (cv * cv);
+    Rb += gb * cp / (cv * cv);
+    Tb += cpb * dcp;
+    // e = e_s(T, Y): de/dT = cv, de/dY_k = e_s,k
+#pragma unroll
+    for (int k = 0; k < ns; k++) {
+        const double esk = nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k];
+        ysb[k] += eb * esk + cpb * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] + Rb * kRuniv * P.inv_mw[k];
+    }
+    Tb += eb * cv;
+    nasa_temperature_vjp<DIM, NSMAX>(P, ns, U, ys, T, Tb, ysb, Ub);
+    fill_y_vjp<NSMAX>(ns, rho, U + 2 + DIM, ysb, Ub, Ub + 2 + DIM);
+}
+
+// reverse of cp_at (conductivity of Sutherland / constant-Lewis transport)
+template <int DIM, int NSMAX>
+ABL_HD void cp_at_vjp(const Phys& P, int ns, const double* U, double T, double cpb, double* Ub, double* Tb) {
+    if (NSMAX == 0 || P.eos == ABL_EOS_PERFECT_GAS) return;
+    constexpr int NY = NSMAX > 0 ? NSMAX : 1;
+    double ys[NY], ysb[NY];
+    fill_y(ns, U[0], U + 2 + DIM, ys);
+    double dcp = 0;
+#pragma unroll
+    for (int k = 0; k < ns; k++) {
+        dcp += ys[k] * nasa_dcp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
+        ysb[k] = cpb * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
+    }
+    *Tb += cpb * dcp;
+    fill_y_vjp<NSMAX>(ns, U[0], U + 2 + DIM, ysb, Ub, Ub + 2 + DIM);
+}
+
+// reverse of transport(): adjoints of mu, k, D into the face state and the face temperature
+template <int DIM, int NSMAX>
+ABL_HD void transport_vjp(const Phys& P, int ns, const double* U, double T, double mub, double kb, double Db, double* Ub, double* Tb) {
+    switch (P.transport) {
+        case ABL_TRANSPORT_SUTHERLAND: {
+            const double pr = 0.707, sc = 0.707, so = 111.0;
+            const double m = sutherland_mu(T);
+            const double cp = cp_at<DIM, NSMAX>(P, ns, U, T);
+            const double mb = mub + kb * cp / pr + Db / (U[0] * sc);
+            Ub[0] -= Db * m / (U[0] * U[0] * sc);
+            *Tb += mb * m * (1.5 / T - 1.0 / (T + so));
+            cp_at_vjp<DIM, NSMAX>(P, ns, U, T, kb * m / pr, Ub, Tb);
+            return;
+        }
+        case ABL_TRANSPORT_CONSTANT_LEWIS: {
+            const double cp = cp_at<DIM, NSMAX>(P, ns, U, T);
+            const double k = P.mu * cp / P.k;
+            const double D = k / (U[0] * cp * P.diff);
+            const double kbt = kb + Db / (U[0] * cp * P.diff);
+            Ub[0] -= Db * D / U[0];
+            cp_at_vjp<DIM, NSMAX>(P, ns, U, T, kbt * P.mu / P.k - Db * D / cp, Ub, Tb);
+            return;
+        }
+        default:
+            return;  // constant properties
+    }
+}
+
+// reverse of cell_aux(): aux = (T, u, Y) of a cell from its conserved state
+template <int DIM, int NS>
+__device__ __forceinline__ void cell_aux_vjp(const Phys& P, const double* u, const double* __restrict__ aux, int c, const double* ab, double* Ub) {
+    using D = Dims<DIM, NS>;
+    const double irho = rcp64(u[0]);
+    double irhob = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        Ub[2 + d] += ab[1 + d] * irho;
+        irhob += ab[1 + d] * u[2 + d];
+    }
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        Ub[D::NE + s] += ab[1 + DIM + s] * irho;
+        irhob += ab[1 + DIM + s] * u[D::NE + s];
+    }
+    Ub[0] -= irhob * irho * irho;
+    if (ab[0] == 0.0) return;
+    if (NS > 0 && P.eos == ABL_EOS_NASA7) {
+        constexpr int NY = NS > 0 ? NS : 1;
+        double ys[NY], ysb[NY];
+        fill_y(NS, u[0], u + D::NE, ys);
+        bool ok = true;
+        const double T = temperature<DIM, NS>(P, NS, u, __ldg(aux + (size_t)c * D::NA), &ok);
+#pragma unroll
+        for (int k = 0; k < NS; k++) ysb[k] = 0.0;
+        nasa_temperature_vjp<DIM, NS>(P, NS, u, ys, T, ab[0], ysb, Ub);
+        fill_y_vjp<NS>(NS, u[0], u + D::NE, ysb, Ub, Ub + D::NE);
+    } else {
+        internal_energy_vjp<DIM>(u, ab[0] * rcp64(P.r_gas / (P.gamma - 1.0)), Ub);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// flux calculators: g[0..7] += d(mf, p12)/d(uL, aL, rhoL, pL, uR, aR, rhoR, pR)^T (mfb, p12b)
+// ---------------------------------------------------------------------------------------------------
+ABL_HD double sgn1(double m) { return m < 0 ? -1.0 : 1.0; }  // the derivative of dabs()
+
+ABL_HD void ausm_vjp(const double* x, double mfb, double p12b, double* g) {
+    const double uL = x[0], aL = x[1], rhoL = x[2], pL = x[3], uR = x[4], aR = x[5], rhoR = x[6], pR = x[7];
+    const double iaR = rcp64(aR), iaL = rcp64(aL);
+    const double Mm = uR * iaR, Mp = uL * iaL;
+    const bool inM = fabs(Mm) <= 1.0, inP = fabs(Mp) <= 1.0;
+    double sMm, sPm, sMp, sPp;
+    if (inM) {
+        sMm = -0.25 * sqr(Mm - 1.0);
+        sPm = -sMm * (2.0 + Mm);
+    } else {
+        sMm = 0.5 * (Mm - fabs(Mm));
+        sPm = sMm / Mm;
+    }
+    if (inP) {
+        sMp = 0.25 * sqr(Mp + 1.0);
+        sPp = sMp * (2.0 - Mp);
+    } else {
+        sMp = 0.5 * (Mp + fabs(Mp));
+        sPp = sMp / Mp;
+    }
+    const double m = sMm + sMp;
+    const double sPmb = p12b * pR, sPpb = p12b * pL;
+    g[7] += p12b * sPm;
+    g[3] += p12b * sPp;
+    double mb;
+    if (m < 0) {
+        mb = mfb * aR * rhoR;
+        g[5] += mfb * m * rhoR;
+        g[6] += mfb * m * aR;
+    } else {
+        mb = mfb * aL * rhoL;
+        g[1] += mfb * m * rhoL;
+        g[2] += mfb * m * aL;
+    }
+    double sMmb = mb, sMpb = mb, Mmb = 0, Mpb = 0;
+    if (inM) {
+        sMmb -= sPmb * (2.0 + Mm);
+        Mmb -= sPmb * sMm;
+        Mmb -= sMmb * 0.5 * (Mm - 1.0);
+    } else {
+        sMmb += sPmb / Mm;
+        Mmb -= sPmb * sPm / Mm;
+        Mmb += sMmb * 0.5 * (1.0 - sgn1(Mm));
+    }
+    if (inP) {
+        sMpb += sPpb * (2.0 - Mp);
+        Mpb -= sPpb * sMp;
+        Mpb += sMpb * 0.5 * (Mp + 1.0);
+    } else {
+        sMpb += sPpb / Mp;
+        Mpb -= sPpb * sPp / Mp;
+        Mpb += sMpb * 0.5 * (1.0 + sgn1(Mp));
+    }
+    g[4] += Mmb * iaR;
+    g[5] -= Mmb * Mm * iaR;
+    g[0] += Mpb * iaL;
+    g[1] -= Mpb * Mp * iaL;
+}
+
+// derivatives of the AUSM+up splitting polynomials (Ausmpup in fv_physics.cuh)
+struct AusmpupD {
+    static ABL_HD double M2P(double m) { return 0.25 * sqr(m + 1.0); }
+    static ABL_HD double M2M(double m) { return -0.25 * sqr(m - 1.0); }
+    static ABL_HD double dM2P(double m) { return 0.5 * (m + 1.0); }
+    static ABL_HD double dM2M(double m) { return -0.5 * (m - 1.0); }
+    static ABL_HD double dM4P(double m) {
+        if (fabs(m) >= 1.0) return 0.5 * (1.0 + sgn1(m));
+        return dM2P(m) * (1.0 - 2.0 * M2M(m)) - 2.0 * M2P(m) * dM2M(m);
+    }
+    static ABL_HD double dM4M(double m) {
+        if (fabs(m) >= 1.0) return 0.5 * (1.0 - sgn1(m));
+        return dM2M(m) * (1.0 + 2.0 * M2P(m)) + 2.0 * M2M(m) * dM2P(m);
+    }
+    // d/dm and d/dfa of P5P, P5M
+    static ABL_HD void dP5P(double m, double fa, double* dm, double* dfa) {
+        if (fabs(m) >= 1.0) {
+            const double e = m + 1E-30, m1 = 0.5 * (m + fabs(m));
+            *dm = (0.5 * (1.0 + sgn1(m)) * e - m1) / (e * e);
+            *dfa = 0.0;
+            return;
+        }
+        const double al = 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa);
+        const double B = (2.0 - m) - 16.0 * al * m * M2M(m);
+        *dm = dM2P(m) * B + M2P(m) * (-1.0 - 16.0 * al * (M2M(m) + m * dM2M(m)));
+        *dfa = -30.0 * fa * m * M2P(m) * M2M(m);
+    }
+    static ABL_HD void dP5M(double m, double fa, double* dm, double* dfa) {
+        if (fabs(m) >= 1.0) {
+            const double e = m + 1E-30, m1 = 0.5 * (m - fabs(m));
+            *dm = (0.5 * (1.0 - sgn1(m)) * e - m1) / (e * e);
+            *dfa = 0.0;
+            return;
+        }
+        const double al = 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa);
+        const double B = (-2.0 - m) + 16.0 * al * m * M2P(m);
+        *dm = dM2M(m) * B + M2M(m) * (-1.0 + 16.0 * al * (M2P(m) + m * dM2P(m)));
+        *dfa = 30.0 * fa * m * M2M(m) * M2P(m);
+    }
+};
+
+ABL_HD void ausmpup_vjp(double mInf, double alpha, const double* x, double mfb, double p12b, double* g) {
+    using A = Ausmpup<double>;
+    using B = AusmpupD;
+    const double uL = x[0], aL = x[1], rhoL = x[2], pL = x[3], uR = x[4], aR = x[5], rhoR = x[6], pR = x[7];
+    const double Kp = 0.25, Ku = 0.75, sigma = 0.25;
+    // forward
+    const double rho12 = 0.5 * (rhoL + rhoR);
+    const double ialpha = rcp64(alpha);
+    const double a12 = 0.5 * (aL + aR) * ialpha;
+    const double ia12 = rcp64(a12);
+    const double mL = uL * ia12, mR = uR * ia12;
+    const double mBar2 = (sqr(uL) + sqr(uR)) * (0.5 * ia12 * ia12);
+    double fa = 1.0, mO = 0.0, xmax = 0.0;
+    const double mInf2 = sqr(mInf);
+    if (mInf > 0) {
+        xmax = pmax(mBar2, mInf2);
+        mO = sqrt(pmin(1.0, xmax));
+        fa = mO * (2.0 - mO);
+    }
+    const double a2 = alpha * alpha;
+    const double c = Kp * rcp64(fa);
+    const double w1 = 1.0 - sigma * mBar2;
+    const double w = pmax(w1, 0.0);
+    const double dp = pR - pL;
+    const double den = rho12 * a12 * a12 * a2;
+    const double idn = rcp64(den);
+    const double m12 = A::M4P(mL) + A::M4M(mR) - c * w * dp * idn;
+    const double p5P = A::P5P(mL, fa), p5M = A::P5M(mR, fa);
+    // reverse
+    double mLb = 0, mRb = 0, fab = 0, a12b = 0, rho12b = 0, mBar2b = 0;
+    const double vb = p12b * rcp64(sqr(alpha));
+    g[3] += vb * p5P;
+    g[7] += vb * p5M;
+    const double K = Ku * rho12 * fa * a12 * a12 * a2 * (mR - mL);
+    const double p5Pb = vb * (pL - p5M * K), p5Mb = vb * (pR - p5P * K);
+    const double Q = -vb * Ku * p5P * p5M * a2;
+    rho12b += Q * fa * a12 * a12 * (mR - mL);
+    fab += Q * rho12 * a12 * a12 * (mR - mL);
+    a12b += Q * rho12 * fa * 2.0 * a12 * (mR - mL);
+    mRb += Q * rho12 * fa * a12 * a12;
+    mLb -= Q * rho12 * fa * a12 * a12;
+    double dm, dfa;
+    B::dP5P(mL, fa, &dm, &dfa);
+    mLb += p5Pb * dm;
+    fab += p5Pb * dfa;
+    B::dP5M(mR, fa, &dm, &dfa);
+    mRb += p5Mb * dm;
+    fab += p5Mb * dfa;
+    double m12b;
+    if (m12 > 0) {
+        m12b = mfb * a12 * rhoL;
+        a12b += mfb * m12 * rhoL;
+        g[2] += mfb * a12 * m12;
+    } else {
+        m12b = mfb * a12 * rhoR;
+        a12b += mfb * m12 * rhoR;
+        g[6] += mfb * a12 * m12;
+    }
+    mLb += m12b * B::dM4P(mL);
+    mRb += m12b * B::dM4M(mR);
+    const double tb = -m12b;
+    const double cb = tb * w * dp * idn, wb = tb * c * dp * idn, dpb = tb * c * w * idn, idnb = tb * c * w * dp;
+    const double denb = -idnb * idn * idn;
+    fab -= cb * Kp / (fa * fa);
+    if (!(w1 < 0.0)) mBar2b -= sigma * wb;
+    g[7] += dpb;
+    g[3] -= dpb;
+    rho12b += denb * a12 * a12 * a2;
+    a12b += denb * rho12 * 2.0 * a12 * a2;
+    if (mInf > 0) {
+        const double mOb = fab * (2.0 - 2.0 * mO);
+        const double mO2b = mO > 0 ? mOb / (2.0 * mO) : 0.0;
+        if (!(1.0 < xmax) && !(mBar2 < mInf2)) mBar2b += mO2b;
+    }
+    double ia12b = mBar2b * (sqr(uL) + sqr(uR)) * ia12;
+    g[0] += mBar2b * uL * ia12 * ia12 + mLb * ia12;
+    g[4] += mBar2b * uR * ia12 * ia12 + mRb * ia12;
+    ia12b += mLb * uL + mRb * uR;
+    a12b -= ia12b * ia12 * ia12;
+    g[1] += 0.5 * a12b * ialpha;
+    g[5] += 0.5 * a12b * ialpha;
+    g[2] += 0.5 * rho12b;
+    g[6] += 0.5 * rho12b;
+}
+
+// any calculator: eight tangent evaluations (exact Riemann, average)
+ABL_HD void calc_vjp_tangents(const Phys& P, const double* x, double mfb, double p12b, double* g, bool* rok) {
+#pragma unroll 1
+    for (int i = 0; i < 8; i++) {
+        Dual xi[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) xi[j] = Dual(x[j], i == j ? 1.0 : 0.0);
+        Dual mf, p12;
+        flux_calc<Dual>(P, xi[0], xi[1], xi[2], xi[3], xi[4], xi[5], xi[6], xi[7], &mf, &p12, rok);
+        g[i] += mfb * mf.d + p12b * p12.d;
+    }
+}
+
+template <int FK>
+ABL_HD void calc_vjp(const Phys& P, const double* x, double mfb, double p12b, double* g, bool* rok) {
+    const int kind = FK >= 0 ? FK : P.flux;
+    if (kind == ABL_FLUX_AUSM)
+        ausm_vjp(x, mfb, p12b, g);
+    else if (kind == ABL_FLUX_AUSMPUP)
+        ausmpup_vjp(P.minf, P.alpha, x, mfb, p12b, g);
+    else
+        calc_vjp_tangents(P, x, mfb, p12b, g, rok);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// face fluxes backwards
+// ---------------------------------------------------------------------------------------------------
+// advection (NavierStokesTransport::AdvectionFlux + SpeciesTransport::AdvectionFlux): fb = flux
+// adjoint, ubL/ubR += adjoints of the two projected face states
+template <int DIM, int NS, int FK>
+__device__ __forceinline__ void advection_vjp(const Phys& P, const double* normal, const double* uL, const double* uR, double TL, double TR, bool adv,
+                                              bool spadv, const double* fb, double* ubL, double* ubR, bool* ok, bool* rok) {
+    using D = Dims<DIM, NS>;
+    double areaMag = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) areaMag += normal[d] * normal[d];
+    areaMag = sqrt(areaMag);
+    const double iA = rcp64(areaMag);
+    double norm[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) norm[d] = normal[d] * iA;
+    const auto dL = decode<DIM, NS>(P, NS, uL, TL * .67 + .33 * TR, ok);
+    const auto dR = decode<DIM, NS>(P, NS, uR, TL * .33 + .67 * TR, ok);
+    const double rhoL = uL[0], rhoR = uR[0];
+    const double irhoL = rcp64(rhoL), irhoR = rcp64(rhoR);
+    double velL[DIM], velR[DIM], unL = 0, unR = 0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        velL[d] = uL[2 + d] * irhoL;
+        unL += velL[d] * norm[d];
+        velR[d] = uR[2 + d] * irhoR;
+        unR += velR[d] * norm[d];
+    }
+    double mf, p12;
+    const int dir = flux_calc_k<FK, double>(P, unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p, &mf, &p12, rok);
+    const double mA = mf * areaMag;
+    double mfb = 0, p12b = 0, ebL = 0, ebR = 0, pbL = 0, pbR = 0, irhobL = 0, irhobR = 0;
+    double velbL[DIM], velbR[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) velbL[d] = velbR[d] = 0.0;
+    if (adv) {
+        mfb += areaMag * fb[0];
+#pragma unroll
+        for (int n = 0; n < DIM; n++) p12b += normal[n] * fb[2 + n];
+        double v2L = 0, v2R = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            v2L += velL[d] * velL[d];
+            v2R += velR[d] * velR[d];
+        }
+        const double mL = sqrt(v2L), mR = sqrt(v2R);
+        const double HL = dL.e + mL * mL / 2.0 + dL.p * irhoL;
+        const double HR = dR.e + mR * mR / 2.0 + dR.p * irhoR;
+        if (dir == ABL_DIR_LEFT || dir == ABL_DIR_RIGHT) {
+            const bool left = dir == ABL_DIR_LEFT;
+            const double H = left ? HL : HR;
+            const double* vel = left ? velL : velR;
+            double s = H * fb[1];
+#pragma unroll
+            for (int n = 0; n < DIM; n++) s += vel[n] * fb[2 + n];
+            mfb += areaMag * s;
+            const double Hb = mA * fb[1];
+            if (left) {
+                ebL += Hb;
+                pbL += Hb * irhoL;
+                irhobL += Hb * dL.p;
+#pragma unroll
+                for (int n = 0; n < DIM; n++) velbL[n] += Hb * velL[n] + mA * fb[2 + n];
+            } else {
+                ebR += Hb;
+                pbR += Hb * irhoR;
+                irhobR += Hb * dR.p;
+#pragma unroll
+                for (int n = 0; n < DIM; n++) velbR[n] += Hb * velR[n] + mA * fb[2 + n];
+            }
+        } else {
+            double s = 0.5 * (HL + HR) * fb[1];
+#pragma unroll
+            for (int n = 0; n < DIM; n++) s += 0.5 * (velL[n] + velR[n]) * fb[2 + n];
+            mfb += areaMag * s;
+            const double Hb = 0.5 * mA * fb[1];
+            ebL += Hb;
+            pbL += Hb * irhoL;
+            irhobL += Hb * dL.p;
+            ebR += Hb;
+            pbR += Hb * irhoR;
+            irhobR += Hb * dR.p;
+#pragma unroll
+            for (int n = 0; n < DIM; n++) {
+                velbL[n] += Hb * velL[n] + 0.5 * mA * fb[2 + n];
+                velbR[n] += Hb * velR[n] + 0.5 * mA * fb[2 + n];
+            }
+        }
+    }
+    if (NS > 0 && spadv) {
+        // LEFT upwinds the left state, anything else the right one
+        const bool left = dir == ABL_DIR_LEFT;
+        const double* u = left ? uL : uR;
+        const double irho = left ? irhoL : irhoR;
+        double* ub = left ? ubL : ubR;
+        double irb = 0;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            mfb += areaMag * u[D::NE + s] * irho * fb[D::NE + s];
+            const double Yb = mA * fb[D::NE + s];
+            ub[D::NE + s] += Yb * irho;
+            irb += Yb * u[D::NE + s];
+        }
+        if (left)
+            irhobL += irb;
+        else
+            irhobR += irb;
+    }
+    double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (mfb != 0.0 || p12b != 0.0) {
+        const double x[8] = {unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p};
+        calc_vjp<FK>(P, x, mfb, p12b, g, rok);
+    }
+    ubL[0] += g[2];
+    ubR[0] += g[6];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        velbL[d] += g[0] * norm[d];
+        velbR[d] += g[4] * norm[d];
+        ubL[2 + d] += velbL[d] * irhoL;
+        irhobL += velbL[d] * uL[2 + d];
+        ubR[2 + d] += velbR[d] * irhoR;
+        irhobR += velbR[d] * uR[2 + d];
+    }
+    ubL[0] -= irhobL * irhoL * irhoL;
+    ubR[0] -= irhobR * irhoR * irhoR;
+    decode_vjp<DIM, NS>(P, NS, uL, dL, ebL, g[1], pbL + g[3], ubL);
+    decode_vjp<DIM, NS>(P, NS, uR, dR, ebR, g[5], pbR + g[7], ubR);
+}
+
+// diffusion (NavierStokesTransport::DiffusionFlux, SpeciesTransport diffusion) backwards: the face
+// state/aux are averages of the two cells and the face gradient the average of their aux gradients,
+// so each side receives half of fsb, fab, gfb
+template <int DIM, int NS>
+__device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* normal, const double* cL, const double* cR, const double* aL,
+                                              const double* aR, const double* gL, const double* gR, bool dif, bool spdif, const double* fb,
+                                              double* fsb, double* fab, double* gfb) {
+    using D = Dims<DIM, NS>;
+    double fs[D::NC], fa[D::NA];
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        fs[k] = cL[k] * 0.5 + cR[k] * 0.5;
+        fsb[k] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < D::NA; k++) {
+        fa[k] = aL[k] * 0.5 + aR[k] * 0.5;
+        fab[k] = 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < D::NA * DIM; k++) gfb[k] = 0.0;
+    double mu, kc, diff;
+    transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
+    double mub = 0, kb = 0, Db = 0;
+    if (dif) {
+        double gv[DIM * DIM], gT[DIM];
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) gv[i] = 0.5 * gL[DIM + i] + 0.5 * gR[DIM + i];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) gT[d] = 0.5 * gL[d] + 0.5 * gR[d];
+        double divVel = 0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) divVel += gv[c * DIM + c];
+        double tau[DIM * DIM], taub[DIM * DIM];
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                tau[c * DIM + d] = (d == c) ? 2.0 * mu * (gv[c * DIM + d] - divVel / 3.0) : mu * (gv[c * DIM + d] + gv[d * DIM + c]);
+                taub[c * DIM + d] = -normal[d] * fb[2 + c];
+            }
+        // energy: -sum_d n_d (sum_c u_c tau_dc + k dT/dx_d)
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+                taub[d * DIM + c] -= normal[d] * fa[1 + c] * fb[1];
+                fab[1 + c] -= normal[d] * tau[d * DIM + c] * fb[1];
+            }
+            kb -= normal[d] * gT[d] * fb[1];
+            gfb[d] -= normal[d] * kc * fb[1];
+        }
+        double gvb[DIM * DIM], divb = 0;
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) gvb[i] = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c)
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                const double tb = taub[c * DIM + d];
+                if (c == d) {
+                    gvb[c * DIM + c] += 2.0 * mu * tb;
+                    divb -= 2.0 * mu / 3.0 * tb;
+                    mub += 2.0 * tb * (gv[c * DIM + c] - divVel / 3.0);
+                } else {
+                    gvb[c * DIM + d] += mu * tb;
+                    gvb[d * DIM + c] += mu * tb;
+                    mub += tb * (gv[c * DIM + d] + gv[d * DIM + c]);
+                }
+            }
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) gvb[c * DIM + c] += divb;
+#pragma unroll
+        for (int i = 0; i < DIM * DIM; i++) gfb[DIM + i] += gvb[i];
+    }
+    if constexpr (NS > 0) {
+        if (spdif) {
+            const double density = fs[0];
+            const int yoff = (1 + DIM) * DIM;
+            double rhob = 0, Tb = 0;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const double hs = P.eos == ABL_EOS_NASA7 ? nasa_h_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s] - P.href[s] : 0.0;
+                double hsb = 0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) {
+                    const double gy = 0.5 * gL[yoff + s * DIM + d] + 0.5 * gR[yoff + s * DIM + d];
+                    const double q = -normal[d] * (fb[D::NE + s] + hs * fb[1]);
+                    rhob += q * diff * gy;
+                    Db += q * density * gy;
+                    gfb[yoff + s * DIM + d] += q * density * diff;
+                    hsb -= normal[d] * density * diff * gy * fb[1];
+                }
+                if (P.eos == ABL_EOS_NASA7) Tb += hsb * nasa_cp_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s];
+            }
+            fsb[0] += rhob;
+            fab[0] += Tb;
+        }
+    }
+    transport_vjp<DIM, NS>(P, NS, fs, fa[0], mub, kb, Db, fsb, &fab[0]);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// per-cell accumulators: [state NC][limited gradient NC*DIM][aux NA][aux gradient NA*DIM]
+template <int DIM, int NS>
+struct AdjRow {
+    using D = Dims<DIM, NS>;
+    static constexpr int U = 0, G = D::NC, A = D::NC + D::NC * DIM, GA = D::NC + D::NC * DIM + D::NA;
+    static constexpr int N = GA + D::NA * DIM;
+};
+
+// one face backwards: the adjoint contributions are added into each side's accumulator row (dst[0]
+// left, dst[1] right; nullptr drops a side that another tile accumulates)
+template <int DIM, int NS, int FK>
+__device__ __forceinline__ void face_vjp(const DevMesh& M, const Phys& P, int L, int R, const double* normal, const double* fdx,
+                                         const double* __restrict__ U, const double* __restrict__ aux, const double* __restrict__ grad,
+                                         const double* __restrict__ agrad, const double* __restrict__ Fb, double* dstL, double* dstR,
+                                         bool* ok, bool* rok) {
+    using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, double>;
+    using AR = AdjRow<DIM, NS>;
+    // dF_L/dflux = -1/V_L, dF_R/dflux = +1/V_R on owned cells
+    double fb[D::NC];
+    const bool oL = M.kind[L] == ABL_CELL_OWNED, oR = M.kind[R] == ABL_CELL_OWNED;
+    const double ivL = oL ? M.ivol[L] : 0.0, ivR = oR ? M.ivol[R] : 0.0;
+#pragma unroll
+    for (int k = 0; k < D::NC; k++)
+        fb[k] = (oR ? __ldg(Fb + (size_t)R * D::NC + k) * ivR : 0.0) - (oL ? __ldg(Fb + (size_t)L * D::NC + k) * ivL : 0.0);
+    double cL[D::NC], cR[D::NC];
+    load_state<DIM, NS>(U, L, cL);
+    load_state<DIM, NS>(U, R, cR);
+    const bool adv = P.advection && P.flux != ABL_FLUX_OFF;
+    const bool spadv = NS > 0 && P.sp_adv && P.flux != ABL_FLUX_OFF;
+    if (adv || spadv) {
+        const bool lsq = P.recon == ABL_RECON_LEASTSQUARES;
+        double uL[D::NC], uR[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) {
+            uL[k] = cL[k];
+            uR[k] = cR[k];
+        }
+        if (lsq) {
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) {
+                double gl[DIM], gr[DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    gl[d] = __ldg(grad + (size_t)L * GR::GS + k * DIM + d);
+                    gr[d] = __ldg(grad + (size_t)R * GR::GS + k * DIM + d);
+                }
+                double dotL = 0, dotR = 0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) {
+                    dotL += gl[d] * fdx[d];
+                    dotR += gr[d] * fdx[3 + d];
+                }
+                uL[k] = uL[k] + dotL;
+                uR[k] = uR[k] + dotR;
+            }
+        }
+        double TL = 300.0, TR = 300.0;
+        if (NS > 0 && P.eos == ABL_EOS_NASA7) {
+            TL = __ldg(aux + (size_t)L * D::NA);
+            TR = __ldg(aux + (size_t)R * D::NA);
+        }
+        double ubL[D::NC], ubR[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) ubL[k] = ubR[k] = 0.0;
+        advection_vjp<DIM, NS, FK>(P, normal, uL, uR, TL, TR, adv, spadv, fb, ubL, ubR, ok, rok);
+        // u_face = u_cell + g . dx: the identity part to the state, the outer product with dx to the gradient
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) {
+            if (dstL) {
+                dstL[AR::U + k] += ubL[k];
+                if (lsq)
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) dstL[AR::G + k * DIM + d] += ubL[k] * fdx[d];
+            }
+            if (dstR) {
+                dstR[AR::U + k] += ubR[k];
+                if (lsq)
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) dstR[AR::G + k * DIM + d] += ubR[k] * fdx[3 + d];
+            }
+        }
+    }
+    const bool dif = P.diffusion && P.transport != ABL_TRANSPORT_NONE;
+    const bool spdif = NS > 0 && P.sp_dif && P.transport != ABL_TRANSPORT_NONE;
+    if (dif || spdif) {
+        double aL[D::NA], aR[D::NA];
+        cell_aux<DIM, NS>(P, cL, aux, L, aL);
+        cell_aux<DIM, NS>(P, cR, aux, R, aR);
+        double gL[D::NA * DIM], gR[D::NA * DIM];
+        load_row<D::NA * DIM, double>(agrad + (size_t)L * GR::AS, gL);
+        load_row<D::NA * DIM, double>(agrad + (size_t)R * GR::AS, gR);
+        double fsb[D::NC], fab[D::NA], gfb[D::NA * DIM];
+        diffusion_vjp<DIM, NS>(P, normal, cL, cR, aL, aR, gL, gR, dif, spdif, fb, fsb, fab, gfb);
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+            double* dst = s == 0 ? dstL : dstR;
+            if (!dst) continue;
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) dst[AR::U + k] += 0.5 * fsb[k];
+#pragma unroll
+            for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k];
+#pragma unroll
+            for (int k = 0; k < D::NA * DIM; k++) dst[AR::GA + k] += 0.5 * gfb[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// cell step: limiter and least-squares gradient backwards (the limiter recomputed), aux-gradient self
+// term; writes the per-cell records the gather reads
+template <int DIM, int NS>
+struct AdjOut {
+    double* gb;     // [nc][GS] adjoint of the unlimited state gradient
+    double* beta;   // [nc][NC] limiter term for the minimising neighbour
+    int* fstar;     // [nc][NC] face of that neighbour, -1 for none
+    double* gab;    // [nc][AS] adjoint of the aux gradient
+    double* ub;     // [nc][NC] state adjoint, own terms
+    double* ab;     // [nc][NA] aux adjoint, own terms
+};
+
+template <int DIM, int NS, int LIM>
+__device__ __forceinline__ void limit_field_vjp(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U, const double* uc,
+                                                const double* g, const double* gtb, double* gbar, double* ub, double* beta, int* fstar, int k0,
+                                                int k1) {
+    using D = Dims<DIM, NS>;
+    double phi[D::NC];
+    int ist[D::NC];
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        phi[k] = DBL_MAX;
+        ist[k] = -1;
+    }
+#pragma unroll 1
+    for (int i = beg; i < end; i++) {
+        const int2 ce = M.cone[i];
+        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+        double v[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) v[d] = __ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d);
+        double un[D::NC];
+        load_state<DIM, NS>(U, n, un);
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) {
+            if (k < k0 || k >= k1) continue;
+            double denom = 0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) denom += g[k * DIM + d] * v[d];
+            const double flim = 0.5 * (un[k] - uc[k]) * rcp64(denom);
+            const double l = limiter_k<LIM, double>(P.limiter, flim);
+            if (!(phi[k] < l)) {  // pmin(phi, l) takes l
+                phi[k] = l;
+                ist[k] = i;
+            }
+        }
+    }
+    bool cancel = false;
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        if (k < k0 || k >= k1) continue;
+        if (phi[k] == 0.0)
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+                if (fabs(g[k * DIM + d]) > P.max_lim_grad) cancel = true;
+    }
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        if (k < k0 || k >= k1) continue;
+        double phib = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            gbar[k * DIM + d] = cancel ? 0.0 : phi[k] * gtb[k * DIM + d];
+            phib += gtb[k * DIM + d] * g[k * DIM + d];
+        }
+        if (cancel || ist[k] < 0 || phib == 0.0) continue;
+        const int2 ce = M.cone[ist[k]];
+        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+        double v[DIM], denom = 0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            v[d] = __ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d);
+            denom += g[k * DIM + d] * v[d];
+        }
+        const double idn = rcp64(denom);
+        const double r = 0.5 * (__ldg(U + (size_t)n * D::NC + k) - uc[k]) * idn;
+        const double dl = limiter_k<LIM, Dual>(P.limiter, Dual(r, 1.0)).d;
+        const double rb = dl * phib;
+        if (rb == 0.0 || !isfinite(rb) || !isfinite(r)) continue;
+        const double bk = 0.5 * rb * idn;  // d r / d (u_n - u_c) = 1 / (2 denom)
+        beta[k] = bk;
+        fstar[k] = f;
+        ub[k] -= bk;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) gbar[k * DIM + d] -= r * rb * idn * v[d];  // d r / d denom = -r / denom
+    }
+}
+
+template <int DIM, int NS, int LIM>
+__device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c, const double* __restrict__ U, const double* acc,
+                                         const AdjOut<DIM, NS>& out, bool do_state, bool do_aux) {
+    using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, double>;
+    using AR = AdjRow<DIM, NS>;
+    const uint8_t kind = M.kind[c];
+    const int beg = M.cone_ptr[c], end = M.cone_ptr[c + 1];
+    double ub[D::NC], gbar[D::NC * DIM], beta[D::NC];
+    int fst[D::NC];
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        ub[k] = acc[AR::U + k];
+        beta[k] = 0.0;
+        fst[k] = -1;
+    }
+#pragma unroll
+    for (int k = 0; k < D::NC * DIM; k++) gbar[k] = 0.0;
+    if (do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO)) {
+        double uc[D::NC], g[D::NC * DIM], ws[DIM];
+        load_state<DIM, NS>(U, c, uc);
+#pragma unroll
+        for (int k = 0; k < D::NC * DIM; k++) g[k] = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) ws[d] = 0.0;
+#pragma unroll 1
+        for (int i = beg; i < end; i++) {
+            const int2 ce = M.cone[i];
+            if (ce.y & kConeBoundary) continue;
+            const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+            double w[DIM], un[D::NC];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+                w[d] = __ldg(M.cgrad + 6 * (size_t)f + 3 * sc + d);
+                ws[d] += w[d];
+            }
+            load_state<DIM, NS>(U, n, un);
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) {
+                const double delta = un[k] - uc[k];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) g[k * DIM + d] += w[d] * delta;
+            }
+        }
+        if (P.limiter != ABL_LIMITER_NONE) {
+            limit_field_vjp<DIM, NS, LIM>(M, P, beg, end, U, uc, g, acc + AR::G, gbar, ub, beta, fst, 0, D::NE);
+            if (NS > 0) limit_field_vjp<DIM, NS, LIM>(M, P, beg, end, U, uc, g, acc + AR::G, gbar, ub, beta, fst, D::NE, D::NC);
+        } else {
+#pragma unroll
+            for (int k = 0; k < D::NC * DIM; k++) gbar[k] = acc[AR::G + k];
+        }
+        // g = sum_f w_f (u_n - u_c): the own-cell term
+#pragma unroll
+        for (int k = 0; k < D::NC; k++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) ub[k] -= ws[d] * gbar[k * DIM + d];
+    }
+    double ab[D::NA], gab[D::NA * DIM];
+#pragma unroll
+    for (int k = 0; k < D::NA; k++) ab[k] = acc[AR::A + k];
+    const bool auxg = do_aux && kind != ABL_CELL_HALO_OUTER;
+#pragma unroll
+    for (int k = 0; k < D::NA * DIM; k++) gab[k] = auxg ? acc[AR::GA + k] : 0.0;
+    if (auxg) {
+        double ws[DIM];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) ws[d] = 0.0;
+#pragma unroll 1
+        for (int i = beg; i < end; i++) {
+            const int2 ce = M.cone[i];
+            const int f = ce.x, sc = (ce.y & kConeSide) ? 1 : 0;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) ws[d] += __ldg(M.fgrad + 6 * (size_t)f + 3 * sc + d);
+        }
+#pragma unroll
+        for (int k = 0; k < D::NA; k++)
+#pragma unroll
+            for (int d = 0; d < DIM; d++) ab[k] -= ws[d] * gab[k * DIM + d];
+    }
+    if (out.gb) {
+        double* o = out.gb + (size_t)c * GR::GS;
+#pragma unroll
+        for (int k = 0; k < D::NC * DIM; k++) o[k] = gbar[k];
+    }
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        out.beta[(size_t)c * D::NC + k] = beta[k];
+        out.fstar[(size_t)c * D::NC + k] = fst[k];
+        out.ub[(size_t)c * D::NC + k] = ub[k];
+    }
+    if (out.gab) {
+        double* o = out.gab + (size_t)c * GR::AS;
+#pragma unroll
+        for (int k = 0; k < D::NA * DIM; k++) o[k] = gab[k];
+    }
+#pragma unroll
+    for (int k = 0; k < D::NA; k++) out.ab[(size_t)c * D::NA + k] = ab[k];
+}
+
+// ---------------------------------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------------------------------
+template <int DIM, int NS, int FK, int LIM>
+__global__ void __launch_bounds__(128, 2) k_tile_adjoint(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
+                                                         const double* __restrict__ grad, const double* __restrict__ agrad,
+                                                         const double* __restrict__ Fb, AdjOut<DIM, NS> out, double* __restrict__ nbrec,
+                                                         int do_state, int do_aux, int* status) {
+    using AR = AdjRow<DIM, NS>;
+    extern __shared__ double sacc[];  // [tile cells][AR::N]
+    const int t = blockIdx.x;
+    const int cb = M.tile_cell_ptr[t], nct = M.tile_cell_ptr[t + 1] - cb;
+    for (int i = threadIdx.x; i < nct * AR::N; i += blockDim.x) sacc[i] = 0.0;
+    __syncthreads();
+    bool ok = true, rok = true;
+    const int base = M.col_base[t], ncol = M.col_base[t + 1] - base - 1;
+    for (int q = 0; q < ncol; q++) {
+        const int fe = M.col_start[base + q + 1];
+        for (int i = M.col_start[base + q] + threadIdx.x; i < fe; i += blockDim.x) {
+            const int2 lr = M.tf_cells[i];
+            double normal[DIM], fdx[6];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_normal + 3 * (size_t)i + d);
+#pragma unroll
+            for (int d = 0; d < 6; d++) fdx[d] = __ldg(M.tf_fdx + 6 * (size_t)i + d);
+            // destination rows: this tile's accumulator, the record of a non-owned side, or none
+            const uint32_t slots = M.tf_slot[i];
+            const int nb = M.tf_nb[i];
+            double* dst[2];
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int slot = s == 0 ? int(slots & 0xffff) : int(slots >> 16);
+                dst[s] = nullptr;
+                if (slot != 0xffff)
+                    dst[s] = sacc + (size_t)slot * AR::N;
+                else if (nb >= 0 && M.kind[s == 0 ? lr.x : lr.y] != ABL_CELL_OWNED)
+                    dst[s] = nbrec + (size_t)nb * AR::N;
+            }
+            face_vjp<DIM, NS, FK>(M, P, lr.x, lr.y, normal, fdx, U, aux, grad, agrad, Fb, dst[0], dst[1], &ok, &rok);
+        }
+        __syncthreads();
+    }
+    for (int j = threadIdx.x; j < nct; j += blockDim.x)
+        cell_vjp<DIM, NS, LIM>(M, P, M.tile_cells[cb + j], U, sacc + (size_t)j * AR::N, out, do_state, do_aux);
+    if (!ok) atomicOr(status, kStatusEos);
+    if (!rok) atomicOr(status, kStatusRiemann);
+}
+
+template <int DIM, int NS, int LIM>
+__global__ void __launch_bounds__(128) k_adjoint_nonowned(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ nbrec,
+                                                          AdjOut<DIM, NS> out, int do_state, int do_aux) {
+    using AR = AdjRow<DIM, NS>;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= M.n_nonowned) return;
+    const int c = M.nonowned[j];
+    double acc[AR::N];
+#pragma unroll
+    for (int k = 0; k < AR::N; k++) acc[k] = 0.0;
+    for (int i = M.cone_ptr[c]; i < M.cone_ptr[c + 1]; i++) {
+        const int nb = M.face_nb[M.cone[i].x];
+        if (nb < 0) continue;
+        const double* r = nbrec + (size_t)nb * AR::N;
+#pragma unroll
+        for (int k = 0; k < AR::N; k++) acc[k] += r[k];
+    }
+    cell_vjp<DIM, NS, LIM>(M, P, c, U, acc, out, do_state, do_aux);
+}
+
+template <int DIM, int NS>
+__global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
+                                                        AdjOut<DIM, NS> in, double* __restrict__ Ub, int do_state, int do_aux, int* status) {
+    using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, double>;
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M.n_cells) return;
+    double ub[D::NC], ab[D::NA];
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) ub[k] = in.ub[(size_t)m * D::NC + k];
+#pragma unroll
+    for (int k = 0; k < D::NA; k++) ab[k] = in.ab[(size_t)m * D::NA + k];
+#pragma unroll 1
+    for (int i = M.cone_ptr[m]; i < M.cone_ptr[m + 1]; i++) {
+        const int2 ce = M.cone[i];
+        const int f = ce.x, n = ce.y & kConeNbr, so = (ce.y & kConeSide) ? 0 : 1;  // so: the neighbour's side of f
+        if (do_state) {
+            if (!(ce.y & kConeBoundary)) {
+                double w[DIM], gn[D::NC * DIM];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cgrad + 6 * (size_t)f + 3 * so + d);
+                load_row<D::NC * DIM, double>(in.gb + (size_t)n * GR::GS, gn);
+#pragma unroll
+                for (int k = 0; k < D::NC; k++)
+#pragma unroll
+                    for (int d = 0; d < DIM; d++) ub[k] += w[d] * gn[k * DIM + d];
+            }
+#pragma unroll
+            for (int k = 0; k < D::NC; k++)
+                if (__ldg(in.fstar + (size_t)n * D::NC + k) == f) ub[k] += __ldg(in.beta + (size_t)n * D::NC + k);
+        }
+        if (do_aux) {
+            double w[DIM], gn[D::NA * DIM];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) w[d] = __ldg(M.fgrad + 6 * (size_t)f + 3 * so + d);
+            load_row<D::NA * DIM, double>(in.gab + (size_t)n * GR::AS, gn);
+#pragma unroll
+            for (int k = 0; k < D::NA; k++)
+#pragma unroll
+                for (int d = 0; d < DIM; d++) ab[k] += w[d] * gn[k * DIM + d];
+        }
+    }
+    double u[D::NC];
+    load_state<DIM, NS>(U, m, u);
+    cell_aux_vjp<DIM, NS>(P, u, aux, m, ab, ub);
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) {
+        Ub[(size_t)m * D::NC + k] += ub[k];
+        finite = finite && isfinite(ub[k]);
+    }
+    if (!finite) atomicOr(status, kStatusNaN);
+}
+
+}  // namespace abl

@@ -6,7 +6,7 @@
 #include <stdexcept>
 #include <string>
 
-#include "fv_kernels.cuh"
+#include "fv_adjoint.cuh"
 
 namespace abl {
 
@@ -84,6 +84,10 @@ struct abl_fv {
     abl::DevBuf<double> tf_normal, tf_fdx;
     abl::DevBuf<uint16_t> tc_face;
     int tile_smem = 0;
+    // adjoint: tile face colours and slots, non-owned records
+    abl::DevBuf<int> col_base, col_start, tf_nb, face_nb, nonowned;
+    abl::DevBuf<uint32_t> tf_slot;
+    int tile_max_cells = 0, n_nb = 0;
     // optional per-kernel timing of the last evaluation
     bool profile = false;
     int n_marks = 0;
@@ -94,6 +98,9 @@ struct abl_fv {
     abl::DevBuf<double> grad64, agrad64, gradD, agradD;
     abl::DevBuf<float> grad32, agrad32;
     abl::DevBuf<int> status;
+    // adjoint work buffers, allocated on the first VJP
+    abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb;
+    abl::DevBuf<int> adj_fstar;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;
@@ -117,5 +124,7 @@ template <int DIM, int NS>
 void run_aux(abl_fv* fv, const double* U, cudaStream_t s);
 template <int DIM, int NS>
 void run_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* dF, cudaStream_t s);
+template <int DIM, int NS>
+void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStream_t s);
 
 }  // namespace abl

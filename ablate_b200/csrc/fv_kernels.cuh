@@ -46,6 +46,14 @@ struct DevMesh {
     const double* tf_fdx;     // [ntf][6]
     const int* tc_fptr;
     const uint16_t* tc_face;
+    // adjoint: face colours per tile, tile-local slots, records of faces with a non-owned side
+    const int* col_base;
+    const int* col_start;
+    const uint32_t* tf_slot;
+    const int* tf_nb;
+    const int* face_nb;
+    int n_nonowned;
+    const int* nonowned;  // cells that are not owned (boundary ghosts, halos)
 };
 
 template <int DIM, int NS>

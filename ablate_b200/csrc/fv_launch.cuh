@@ -89,4 +89,54 @@ void run_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* d
     mark(fv, "end", s);
 }
 
+// reverse mode: Ub += (dF/dU)^T Fb with the forward gradients recomputed (k_gradient), the face
+// fluxes run backwards per tile, then the per-cell limiter / gradient / aux steps and their gather
+template <int DIM, int NS>
+void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStream_t s) {
+    using AR = AdjRow<DIM, NS>;
+    const DevMesh& M = fv->mesh;
+    const Phys& P = fv->phys;
+    fv->n_marks = 0;
+    if (fv->need_aux) {
+        mark(fv, "k_aux", s);
+        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, P, U, fv->aux.p, fv->status.p);
+        check_launch();
+    }
+    if (fv->need_state_grad || fv->need_aux_grad) {
+        mark(fv, "k_gradient", s);
+        if (P.limiter == ABL_LIMITER_MINMOD)
+            launch_gradient<DIM, NS, double, ABL_LIMITER_MINMOD>(fv, U, nullptr, fv->grad64.p, fv->agrad64.p, s);
+        else
+            launch_gradient<DIM, NS, double, -1>(fv, U, nullptr, fv->grad64.p, fv->agrad64.p, s);
+    }
+    AdjOut<DIM, NS> out{fv->need_state_grad ? fv->adj_gb.p : nullptr, fv->adj_beta.p, fv->adj_fstar.p,
+                        fv->need_aux_grad ? fv->adj_gab.p : nullptr, fv->adj_ub.p, fv->adj_ab.p};
+    const int ds = fv->need_state_grad, da = fv->need_aux_grad;
+    mark(fv, "k_tile_adjoint", s);
+    if (fv->n_nb > 0) ABL_CUDA(cudaMemsetAsync(fv->adj_nb.p, 0, (size_t)fv->n_nb * AR::N * sizeof(double), s));
+    if (M.n_tiles > 0) {
+        const size_t smem = (size_t)fv->tile_max_cells * AR::N * sizeof(double);
+        if (smem > 227 * 1024) throw AblError(ABL_ERR_UNSUPPORTED, "adjoint accumulators exceed shared memory for this species count");
+        // flux calculator and limiter fixed at compile time where a specialised kernel exists
+        auto kern = k_tile_adjoint<DIM, NS, -1, -1>;
+        if (P.flux == ABL_FLUX_AUSMPUP)
+            kern = P.limiter == ABL_LIMITER_MINMOD ? k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, ABL_LIMITER_MINMOD>
+                                                   : k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, -1>;
+        else if (P.flux == ABL_FLUX_AUSM)
+            kern = k_tile_adjoint<DIM, NS, ABL_FLUX_AUSM, -1>;
+        ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<M.n_tiles, 128, smem, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p, Fb, out, fv->adj_nb.p, ds, da, fv->status.p);
+        check_launch();
+    }
+    mark(fv, "k_adjoint_nonowned", s);
+    if (M.n_nonowned > 0) {
+        k_adjoint_nonowned<DIM, NS, -1><<<blocks_for(M.n_nonowned, 128), 128, 0, s>>>(M, P, U, fv->adj_nb.p, out, ds, da);
+        check_launch();
+    }
+    mark(fv, "k_adjoint_gather", s);
+    k_adjoint_gather<DIM, NS><<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, fv->aux.p, out, Ub, ds, da, fv->status.p);
+    check_launch();
+    mark(fv, "end", s);
+}
+
 }  // namespace abl

@@ -108,9 +108,15 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
 
 // Cell tiles for the fused flux kernel: owned cells sorted along a Morton curve of their centroids
 // and cut into runs of at most `tile_cells` cells (on power-of-two boxes each run is a compact block).
-// Every tile lists all flux faces of its cells (faces shared by two tiles appear in both lists) in
-// ascending global face order, with the face geometry copied into tile order so the kernel streams
-// it, and for every tile cell the (local face, side) pairs in ascending face order.
+// Every tile lists all flux faces of its cells (faces shared by two tiles appear in both lists), with
+// the face geometry copied into tile order so the kernel streams it, and for every tile cell the
+// (local face, side) pairs in ascending global face order.
+//
+// Within a tile the faces are greedily coloured so that no two faces of one colour touch the same
+// tile cell, and stored colour by colour (ascending face order inside a colour). The adjoint kernel
+// accumulates per-cell sums in shared memory one colour at a time, which needs no atomics and fixes
+// the summation order. A face with a side that is not an owned cell (a boundary ghost or a partition
+// halo) is in exactly one tile; its contribution to that side goes to a per-face record (nb index).
 struct Tiles {
     int n_tiles = 0;
     int max_faces = 0;                    // largest per-tile face count (sizes shared memory)
@@ -122,6 +128,13 @@ struct Tiles {
     std::vector<double> tf_fdx;           // [ntf][6] face centroid minus each side's centroid
     std::vector<int32_t> tc_fptr;         // [n_owned+1] per tile cell into tc_face
     std::vector<uint16_t> tc_face;        // local face index | side << 15
+    std::vector<uint32_t> tf_slot;        // [ntf] tile-local slot of L | of R << 16 (0xffff: not a tile cell)
+    std::vector<int32_t> tf_nb;           // [ntf] record of the non-owned side, -1 if both sides are owned
+    std::vector<int32_t> col_base;        // [n_tiles+1] into col_start
+    std::vector<int32_t> col_start;       // per tile: first tile face of each colour, then the end
+    std::vector<int32_t> face_nb;         // [n_faces] record index of faces with a non-owned side, else -1
+    int n_nb = 0;                         // number of such records
+    int max_colors = 0;
 };
 
 inline uint64_t morton_spread(uint64_t x, int dim) {
@@ -170,7 +183,13 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
     std::vector<int32_t> faces;
     t.face_ptr.push_back(0);
     t.tc_fptr.assign(n + 1, 0);
+    t.col_base.push_back(0);
     std::vector<std::vector<uint16_t>> lists;
+    t.face_nb.assign(h.n_faces, -1);
+    for (int f : h.flux_faces)
+        if (h.kind[h.face_cells[2 * f]] != ABL_CELL_OWNED || h.kind[h.face_cells[2 * f + 1]] != ABL_CELL_OWNED) t.face_nb[f] = t.n_nb++;
+    std::vector<uint64_t> used;
+    std::vector<int> color, order, pos;
     for (int k = 0; k < t.n_tiles; k++) {
         const int cb = t.cell_ptr[k], ce = t.cell_ptr[k + 1];
         faces.clear();
@@ -184,15 +203,49 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         if (faces.size() > 0x7fff) throw std::invalid_argument("tile has too many faces");
         t.max_faces = std::max(t.max_faces, (int)faces.size());
         lists.assign(ce - cb, {});
+        // greedy colouring over the tile cells each face touches
+        used.assign(ce - cb, 0);
+        color.assign(faces.size(), 0);
+        int ncol = 0;
         for (size_t i = 0; i < faces.size(); i++) {
+            const int f = faces[i];
+            const int lL = local[h.face_cells[2 * f]], lR = local[h.face_cells[2 * f + 1]];
+            const uint64_t busy = (lL >= 0 ? used[lL] : 0) | (lR >= 0 ? used[lR] : 0);
+            int c = 0;
+            while (c < 64 && (busy >> c) & 1ull) c++;
+            if (c == 64) throw std::invalid_argument("tile face colouring needs more than 64 colours");
+            color[i] = c;
+            ncol = std::max(ncol, c + 1);
+            if (lL >= 0) used[lL] |= 1ull << c;
+            if (lR >= 0) used[lR] |= 1ull << c;
+        }
+        t.max_colors = std::max(t.max_colors, ncol);
+        order.resize(faces.size());
+        for (size_t i = 0; i < faces.size(); i++) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return color[a] < color[b]; });
+        pos.assign(faces.size(), 0);
+        const int base = (int)(t.tf_cells.size() / 2);
+        for (size_t q = 0; q < order.size(); q++) {
+            const int i = order[q];
+            pos[i] = (int)q;
+            if (q == 0 || color[order[q - 1]] != color[i]) t.col_start.push_back(base + (int)q);
             const int f = faces[i];
             const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
             t.tf_cells.push_back(L);
             t.tf_cells.push_back(R);
             for (int d = 0; d < 3; d++) t.tf_normal.push_back(d < dim ? m->face_normal[3 * (size_t)f + d] : 0.0);
-            for (int q = 0; q < 6; q++) t.tf_fdx.push_back(h.fdx[6 * (size_t)f + q]);
-            if (local[L] >= 0) lists[local[L]].push_back((uint16_t)i);
-            if (local[R] >= 0) lists[local[R]].push_back((uint16_t)(i | 0x8000));
+            for (int z = 0; z < 6; z++) t.tf_fdx.push_back(h.fdx[6 * (size_t)f + z]);
+            t.tf_slot.push_back((uint32_t)(local[L] >= 0 ? local[L] : 0xffff) | ((uint32_t)(local[R] >= 0 ? local[R] : 0xffff) << 16));
+            t.tf_nb.push_back(t.face_nb[f]);
+        }
+        t.col_start.push_back(base + (int)order.size());
+        t.col_base.push_back((int)t.col_start.size());
+        // per-cell lists in ascending global face order, pointing at the colour-ordered positions
+        for (size_t i = 0; i < faces.size(); i++) {
+            const int f = faces[i];
+            const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
+            if (local[L] >= 0) lists[local[L]].push_back((uint16_t)pos[i]);
+            if (local[R] >= 0) lists[local[R]].push_back((uint16_t)(pos[i] | 0x8000));
         }
         for (int j = cb; j < ce; j++) {
             t.tc_fptr[j + 1] = t.tc_fptr[j] + (int)lists[j - cb].size();

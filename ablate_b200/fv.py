@@ -343,6 +343,18 @@ class FiniteVolumeSolver:
         L.check(L.lib.abl_fv_jvp(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(dU_ptr), C.c_void_p(F_ptr or None), C.c_void_p(dF_ptr),
                                  C.c_void_p(stream)), "abl_fv_jvp")
 
+    def ComputeVJP(self, time: float, locX: np.ndarray, Fbar: np.ndarray, Ubar: np.ndarray):
+        """Ubar += J(locX)^T Fbar, host arrays (n_cells, nc); Fbar is read on owned cells."""
+        x = np.ascontiguousarray(locX, dtype=np.float64)
+        fb = np.ascontiguousarray(Fbar, dtype=np.float64)
+        assert Ubar.dtype == np.float64 and Ubar.flags.c_contiguous and Ubar.shape == x.shape
+        L.check(L.lib.abl_fv_vjp_host(self.handle, time, L.dptr(x), L.dptr(fb), L.dptr(Ubar)), "abl_fv_vjp_host")
+        return Ubar
+
+    def ComputeVJPDevice(self, time: float, U_ptr: int, Fbar_ptr: int, Ubar_ptr: int, stream: int = 0):
+        L.check(L.lib.abl_fv_vjp(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(Fbar_ptr), C.c_void_p(Ubar_ptr), C.c_void_p(stream)),
+                "abl_fv_vjp")
+
     def UpdateAux(self, locX: np.ndarray):
         """Recompute the aux fields (T, u, Y) from host state locX (CellSolver::UpdateAuxFields)."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

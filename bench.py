@@ -271,24 +271,44 @@ def main():
         solver.Profile(False)
         kernels[prec] = {name: ms / args.steps for name, ms in acc.items()}
 
-    # forward tangent (JVP) cost relative to one FP64 RHS, same protocol
-    jvp_ms = None
+    # forward tangent (JVP) and adjoint (VJP) costs relative to one FP64 RHS, same protocol
+    def timed(fn, what):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            fn()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize(dev)
+        if solver.Status() != L.OK:
+            raise RuntimeError(f"device status after the timed {what}")
+        ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        solver.Profile(True)
+        split: dict = {}
+        for k in range(args.steps):
+            flush.zero_()
+            fn()
+            for name, kms in solver.ProfileRead().items():
+                split[name] = split.get(name, 0.0) + kms / args.steps
+        solver.Profile(False)
+        return ms, split
+
+    jvp_ms = vjp_ms = None
     if L.PRECISION_FP64 in results:
         dU = torch.randn_like(U) * U.abs().mean(0, keepdim=True) * 1e-2
         dF = torch.zeros_like(U)
-        for _ in range(args.warmup):
-            solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream)
-        torch.cuda.synchronize(dev)
-        jev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        for k in range(args.steps):
-            flush.zero_()
-            jev[k][0].record(stream)
-            solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream)
-            jev[k][1].record(stream)
-        torch.cuda.synchronize(dev)
-        jvp_ms = sum(a.elapsed_time(b) for a, b in jev) / args.steps
-        if solver.Status() != L.OK:
-            raise RuntimeError("device status after the timed JVP")
+        jvp_ms, kernels["jvp"] = timed(lambda: solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream), "JVP")
+        Fbar = torch.randn_like(U)
+        Ubar = torch.zeros_like(U)
+        vjp_ms, kernels["vjp"] = timed(lambda: solver.ComputeVJPDevice(0.0, U.data_ptr(), Fbar.data_ptr(), Ubar.data_ptr(), stream.cuda_stream),
+                                       "VJP")
 
     # accuracy of the mixed path against FP64 on this workload
     mixed_err = None
@@ -350,12 +370,13 @@ def main():
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
                      "whole_rhs": {"achieved": achieved, "frac": achieved / peak, "ms": head_ms},
                      "note": "the dominant kernel touches every algorithmic byte of the RHS (state, residual, 1/V, face cells, normals)"},
-        "kernel_ms": {("fp64" if p == L.PRECISION_FP64 else "mixed"): v for p, v in kernels.items()},
+        "kernel_ms": {({L.PRECISION_FP64: "fp64", L.PRECISION_MIXED: "mixed"}.get(p, p)): v for p, v in kernels.items()},
         "precisions": {("fp64" if p == L.PRECISION_FP64 else "mixed"): {"ms_per_step": ms, "mcell_per_s": world * n_cells / (ms * 1e-3) / 1e6,
                                                                           "hbm_gbs": B / (ms * 1e-3) / 1e9}
                        for p, ms in results.items()},
         "mixed_rel_err_vs_fp64": mixed_err,
-        "vjp_over_rhs": None,
+        "vjp_over_rhs": (vjp_ms / results[L.PRECISION_FP64]) if vjp_ms else None,
+        "vjp": {"ms_per_step": vjp_ms, "over_rhs_fp64": (vjp_ms / results[L.PRECISION_FP64]) if vjp_ms else None},
         "jvp": {"ms_per_step": jvp_ms, "over_rhs_fp64": (jvp_ms / results[L.PRECISION_FP64]) if jvp_ms else None},
         "e2e": {"value": world * n_cells / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 2 * state_bytes,
                 "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,

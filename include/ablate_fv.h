@@ -191,6 +191,15 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
 int abl_fv_jvp(abl_fv* fv, double time, const double* U_dev, const double* dU_dev, double* F_dev, double* dF_dev, void* stream);
 int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double* dU_host, double* F_host, double* dF_host);
 
+/* Adjoint (vector-Jacobian product) of abl_fv_rhs at FP64: Ubar += J(U)^T Fbar. Fbar is read on owned
+ * cells (the rows the RHS writes); Ubar receives every cell, boundary ghosts and halos included, since
+ * their values enter the owned residuals. It is the transpose of the abl_fv_jvp tangent (same active
+ * branches). Only the forward gradients are stored; the limiter, EOS decode and fluxes are recomputed.
+ * The reference has no adjoint; it would form J^T only through a finite-difference Jacobian
+ * (SNESComputeJacobianDefaultColor / MatMFFD) of ComputeRHSFunction (finiteVolumeSolver.cpp:233-291). */
+int abl_fv_vjp(abl_fv* fv, double time, const double* U_dev, const double* Fbar_dev, double* Ubar_dev, void* stream);
+int abl_fv_vjp_host(abl_fv* fv, double time, const double* U_host, const double* Fbar_host, double* Ubar_host);
+
 /* Aux fields (T, u, Y). With the NASA-7 mixture EOS every abl_fv_rhs updates them (the resident T is
  * also the next secant guess); with a perfect gas the RHS recomputes them on the fly and they are
  * refreshed only by abl_fv_update_aux. set_aux sets the temperature guess used by the next update. */

@@ -30,13 +30,20 @@ CASES = ["tgv3d_ausmpup_lsq_minmod_visc", "box2d_ausm_upwind_none", "box2d_ausmp
 def _direction(w, seed):
     rng = np.random.default_rng(seed)
     scale = np.abs(w.U).mean(0)
+    scale = np.where(scale > 0, scale, 1e-2 * np.sqrt(scale[0] * scale[1]))  # momentum of a fluid at rest
     dU = rng.standard_normal(w.U.shape) * scale * 1e-2
     dU[w.mesh.cell_kind == L.CELL_BOUNDARY] = 0.0  # boundary ghost values are not unknowns of the RHS
     return dU
 
 
 def _generic(w):
-    U = w.U * (1.0 + 1e-3 * np.random.default_rng(11).standard_normal(w.U.shape))
+    # 0.1% relative noise; vanishing components (the momentum of a fluid at rest) get absolute noise,
+    # which moves the state off the u = 0 switch of the upwind direction
+    rng = np.random.default_rng(11)
+    U = w.U * (1.0 + 1e-3 * rng.standard_normal(w.U.shape))
+    s = np.abs(w.U).mean(0)
+    zero = s == 0
+    U[:, zero] += 1e-5 * np.sqrt(s[0] * s[1]) * rng.standard_normal((w.U.shape[0], int(zero.sum())))
     return np.ascontiguousarray(U)
 
 
