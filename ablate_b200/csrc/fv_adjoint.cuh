@@ -967,8 +967,15 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
 // ---------------------------------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------------------------------
+// resident CTAs per SM the register budget targets (shared memory holds 3 tiles of accumulators at
+// 0 species; the species instances need more of both)
+template <int NS>
+struct AdjBlocks {
+    static constexpr int tile = NS == 0 ? 3 : 2;
+};
+
 template <int DIM, int NS, int FK, int LIM>
-__global__ void __launch_bounds__(128, 2) k_tile_adjoint(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
+__global__ void __launch_bounds__(128, AdjBlocks<NS>::tile) k_tile_adjoint(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
                                                          const double* __restrict__ grad, const double* __restrict__ agrad,
                                                          const double* __restrict__ Fb, AdjOut<DIM, NS> out, double* __restrict__ nbrec,
                                                          int do_state, int do_aux, int* status) {
@@ -982,7 +989,7 @@ __global__ void __launch_bounds__(128, 2) k_tile_adjoint(DevMesh M, Phys P, cons
     const int base = M.col_base[t], ncol = M.col_base[t + 1] - base - 1;
     for (int q = 0; q < ncol; q++) {
         const int fe = M.col_start[base + q + 1];
-        for (int i = M.col_start[base + q] + threadIdx.x; i < fe; i += blockDim.x) {
+        for (int i = M.col_start[base + q] + threadIdx.x; i < fe; i += blockDim.x) {  // one pass: a colour has <= 128 faces
             const int2 lr = M.tf_cells[i];
             double normal[DIM], fdx[6];
 #pragma unroll

@@ -137,6 +137,8 @@ struct Tiles {
     int max_colors = 0;
 };
 
+constexpr int kColorCap = 128;  // faces per colour = threads per CTA of the adjoint tile kernel
+
 inline uint64_t morton_spread(uint64_t x, int dim) {
     if (dim == 1) return x;
     uint64_t r = 0;
@@ -189,7 +191,7 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
     for (int f : h.flux_faces)
         if (h.kind[h.face_cells[2 * f]] != ABL_CELL_OWNED || h.kind[h.face_cells[2 * f + 1]] != ABL_CELL_OWNED) t.face_nb[f] = t.n_nb++;
     std::vector<uint64_t> used;
-    std::vector<int> color, order, pos;
+    std::vector<int> color, order, pos, count;
     for (int k = 0; k < t.n_tiles; k++) {
         const int cb = t.cell_ptr[k], ce = t.cell_ptr[k + 1];
         faces.clear();
@@ -203,18 +205,21 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         if (faces.size() > 0x7fff) throw std::invalid_argument("tile has too many faces");
         t.max_faces = std::max(t.max_faces, (int)faces.size());
         lists.assign(ce - cb, {});
-        // greedy colouring over the tile cells each face touches
+        // greedy colouring over the tile cells each face touches, at most kColorCap faces per colour
+        // (one face per thread of the adjoint kernel's CTA, so every colour is one pass)
         used.assign(ce - cb, 0);
         color.assign(faces.size(), 0);
+        count.assign(64, 0);
         int ncol = 0;
         for (size_t i = 0; i < faces.size(); i++) {
             const int f = faces[i];
             const int lL = local[h.face_cells[2 * f]], lR = local[h.face_cells[2 * f + 1]];
             const uint64_t busy = (lL >= 0 ? used[lL] : 0) | (lR >= 0 ? used[lR] : 0);
             int c = 0;
-            while (c < 64 && (busy >> c) & 1ull) c++;
+            while (c < 64 && (((busy >> c) & 1ull) || count[c] >= kColorCap)) c++;
             if (c == 64) throw std::invalid_argument("tile face colouring needs more than 64 colours");
             color[i] = c;
+            count[c]++;
             ncol = std::max(ncol, c + 1);
             if (lL >= 0) used[lL] |= 1ull << c;
             if (lR >= 0) used[lR] |= 1ull << c;
