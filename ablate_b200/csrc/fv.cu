@@ -393,6 +393,19 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         }
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
+        {
+            // per cell: sum of its LSQ weights over non-boundary faces, and of its aux weights over all
+            std::vector<double> ws((size_t)h.n_cells * 6, 0.0);
+            for (int c = 0; c < h.n_cells; c++)
+                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                    const size_t slot = (size_t)h.cone_face[i] * 6 + 3 * h.cone_side[i];
+                    for (int d = 0; d < h.dim; d++) {
+                        if (lsq && !h.face_boundary[h.cone_face[i]]) ws[6 * (size_t)c + d] += h.cgrad[slot + d];
+                        if (dif) ws[6 * (size_t)c + 3 + d] += h.fgrad[slot + d];
+                    }
+                }
+            fv->wsum.upload(ws.data(), ws.size());
+        }
 
         fv->aux.alloc((size_t)fv->n_cells * fv->naux);
         {
@@ -440,6 +453,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.face_nb = fv->face_nb.p;
         M.n_nonowned = (int)fv->nonowned.n;
         M.nonowned = fv->nonowned.p;
+        M.wsum = fv->wsum.p;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();
     });
@@ -544,6 +558,11 @@ int abl_fv_vjp(abl_fv* fv, double time, const double* U_dev, const double* Fbar_
             fv->adj_ab.alloc(n * fv->naux);
             fv->adj_nb.alloc((size_t)std::max(fv->n_nb, 1) * (fv->nc + fv->nc * fv->dim + fv->naux + fv->naux * fv->dim));
             fv->adj_ub.alloc(n * fv->nc);
+            if (fv->need_state_grad) {
+                fv->adj_graw.alloc(n * round_up(fv->nc * fv->dim, 2));
+                fv->adj_phi.alloc(n * fv->nc);
+                fv->adj_ist.alloc(n * fv->nc);
+            }
         }
         dispatch_vjp(fv, U_dev, Fbar_dev, Ubar_dev, static_cast<cudaStream_t>(stream));
     });

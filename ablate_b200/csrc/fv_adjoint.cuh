@@ -5,16 +5,16 @@
 // transpose of the tangent the dual-number kernels propagate (the derivative of the branch the primal
 // evaluation takes at limiter minima, flux-splitting switches and mass-fraction clips).
 //
-// Nothing of the forward pass is stored beyond what one RHS already keeps: the limited gradients and
-// aux gradients from k_gradient. Every other intermediate is recomputed:
-//   k_gradient          forward gradients (the RHS kernel, unchanged)
+// Of the forward pass only per-cell data is kept: the limited gradients and aux gradients one RHS
+// keeps anyway, plus the unlimited gradient, the limiter factor and the minimising face per component.
+// Every per-face intermediate (face states, EOS decode, flux calculator) is recomputed:
+//   k_gradient          forward gradients, with the limiter records
 //   k_tile_adjoint      one CTA per tile. Per face, colour by colour: recompute the face states, the
 //                       EOS decode and the flux calculator, then run the flux backwards; the adjoint of
 //                       each side's state, limited gradient, aux and aux gradient is summed into that
 //                       cell's shared-memory accumulators (faces of one colour touch distinct cells, so
-//                       no atomics and a fixed order). Then per tile cell: the limiter is recomputed
-//                       (its minimising face per component) and the limiter and least-squares gradient
-//                       are run backwards.
+//                       no atomics and a fixed order). Then per tile cell the limiter and least-squares
+//                       gradient are run backwards from the records of the forward gradient pass.
 //   k_adjoint_nonowned  the same cell step for boundary ghosts and halos, from per-face records.
 //   k_adjoint_gather    per cell: the neighbour terms of the gradient, limiter and aux-gradient adjoints
 //                       (a gather over the cell's faces, the transpose of the forward gathers), then the
@@ -437,11 +437,17 @@ ABL_HD void calc_vjp(const Phys& P, const double* x, double mfb, double p12b, do
 // ---------------------------------------------------------------------------------------------------
 // face fluxes backwards
 // ---------------------------------------------------------------------------------------------------
-// advection (NavierStokesTransport::AdvectionFlux + SpeciesTransport::AdvectionFlux): fb = flux
-// adjoint, ubL/ubR += adjoints of the two projected face states
+// Two lanes per face: lanes 2j (left side) and 2j+1 (right side) of a warp hold one face. Each lane
+// projects, decodes and reverses its own side; what couples the sides (the flux calculator and the
+// upwind choice, the averaged face state of the diffusion flux) is exchanged with the partner lane and
+// evaluated identically in both. Every exchange sits in control flow both lanes take.
+__device__ __forceinline__ double xch(unsigned mask, double v) { return __shfl_xor_sync(mask, v, 1); }
+
+// advection (NavierStokesTransport::AdvectionFlux + SpeciesTransport::AdvectionFlux) backwards for
+// this lane's side: fb = flux adjoint, ub += adjoint of this side's projected face state u
 template <int DIM, int NS, int FK>
-__device__ __forceinline__ void advection_vjp(const Phys& P, const double* normal, const double* uL, const double* uR, double TL, double TR, bool adv,
-                                              bool spadv, const double* fb, double* ubL, double* ubR, bool* ok, bool* rok) {
+__device__ __forceinline__ void advection_vjp_side(const Phys& P, unsigned mask, int side, const double* normal, const double* u, double Tguess,
+                                                   bool adv, bool spadv, const double* fb, double* ub, bool* ok, bool* rok) {
     using D = Dims<DIM, NS>;
     double areaMag = 0;
 #pragma unroll
@@ -451,150 +457,109 @@ __device__ __forceinline__ void advection_vjp(const Phys& P, const double* norma
     double norm[DIM];
 #pragma unroll
     for (int d = 0; d < DIM; d++) norm[d] = normal[d] * iA;
-    const auto dL = decode<DIM, NS>(P, NS, uL, TL * .67 + .33 * TR, ok);
-    const auto dR = decode<DIM, NS>(P, NS, uR, TL * .33 + .67 * TR, ok);
-    const double rhoL = uL[0], rhoR = uR[0];
-    const double irhoL = rcp64(rhoL), irhoR = rcp64(rhoR);
-    double velL[DIM], velR[DIM], unL = 0, unR = 0;
+    const auto dd = decode<DIM, NS>(P, NS, u, Tguess, ok);
+    const double rho = u[0], irho = rcp64(rho);
+    double vel[DIM], un = 0, v2 = 0;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        velL[d] = uL[2 + d] * irhoL;
-        unL += velL[d] * norm[d];
-        velR[d] = uR[2 + d] * irhoR;
-        unR += velR[d] * norm[d];
+        vel[d] = u[2 + d] * irho;
+        un += vel[d] * norm[d];
+        v2 += vel[d] * vel[d];
     }
+    const double vm = sqrt(v2);
+    const double H = dd.e + vm * vm / 2.0 + dd.p * irho;
+    // the flux calculator on both sides' values, in (left, right) order in both lanes
+    const double un_o = xch(mask, un), a_o = xch(mask, dd.a), rho_o = xch(mask, rho), p_o = xch(mask, dd.p);
+    const double x[8] = {side ? un_o : un, side ? a_o : dd.a, side ? rho_o : rho, side ? p_o : dd.p,
+                         side ? un : un_o, side ? dd.a : a_o, side ? rho : rho_o, side ? dd.p : p_o};
     double mf, p12;
-    const int dir = flux_calc_k<FK, double>(P, unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p, &mf, &p12, rok);
+    const int dir = flux_calc_k<FK, double>(P, x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], &mf, &p12, rok);
     const double mA = mf * areaMag;
-    double mfb = 0, p12b = 0, ebL = 0, ebR = 0, pbL = 0, pbR = 0, irhobL = 0, irhobR = 0;
-    double velbL[DIM], velbR[DIM];
+    const double H_o = xch(mask, H);
+    double vel_o[DIM];
 #pragma unroll
-    for (int d = 0; d < DIM; d++) velbL[d] = velbR[d] = 0.0;
+    for (int d = 0; d < DIM; d++) vel_o[d] = xch(mask, vel[d]);
+    // LEFT upwinds side 0, RIGHT side 1; for the species anything but LEFT takes side 1
+    const bool upme = (dir == ABL_DIR_LEFT) == (side == 0);
+    double mfb = 0, p12b = 0, eb = 0, pb = 0, irhob = 0, velb[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) velb[d] = 0.0;
     if (adv) {
         mfb += areaMag * fb[0];
 #pragma unroll
         for (int n = 0; n < DIM; n++) p12b += normal[n] * fb[2 + n];
-        double v2L = 0, v2R = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-            v2L += velL[d] * velL[d];
-            v2R += velR[d] * velR[d];
-        }
-        const double mL = sqrt(v2L), mR = sqrt(v2R);
-        const double HL = dL.e + mL * mL / 2.0 + dL.p * irhoL;
-        const double HR = dR.e + mR * mR / 2.0 + dR.p * irhoR;
         if (dir == ABL_DIR_LEFT || dir == ABL_DIR_RIGHT) {
-            const bool left = dir == ABL_DIR_LEFT;
-            const double H = left ? HL : HR;
-            const double* vel = left ? velL : velR;
-            double s = H * fb[1];
+            double sacc = (upme ? H : H_o) * fb[1];
 #pragma unroll
-            for (int n = 0; n < DIM; n++) s += vel[n] * fb[2 + n];
-            mfb += areaMag * s;
-            const double Hb = mA * fb[1];
-            if (left) {
-                ebL += Hb;
-                pbL += Hb * irhoL;
-                irhobL += Hb * dL.p;
+            for (int n = 0; n < DIM; n++) sacc += (upme ? vel[n] : vel_o[n]) * fb[2 + n];
+            mfb += areaMag * sacc;
+            if (upme) {
+                const double Hb = mA * fb[1];
+                eb += Hb;
+                pb += Hb * irho;
+                irhob += Hb * dd.p;
 #pragma unroll
-                for (int n = 0; n < DIM; n++) velbL[n] += Hb * velL[n] + mA * fb[2 + n];
-            } else {
-                ebR += Hb;
-                pbR += Hb * irhoR;
-                irhobR += Hb * dR.p;
-#pragma unroll
-                for (int n = 0; n < DIM; n++) velbR[n] += Hb * velR[n] + mA * fb[2 + n];
+                for (int n = 0; n < DIM; n++) velb[n] += Hb * vel[n] + mA * fb[2 + n];
             }
         } else {
-            double s = 0.5 * (HL + HR) * fb[1];
+            double sacc = 0.5 * (H + H_o) * fb[1];
 #pragma unroll
-            for (int n = 0; n < DIM; n++) s += 0.5 * (velL[n] + velR[n]) * fb[2 + n];
-            mfb += areaMag * s;
+            for (int n = 0; n < DIM; n++) sacc += 0.5 * (vel[n] + vel_o[n]) * fb[2 + n];
+            mfb += areaMag * sacc;
             const double Hb = 0.5 * mA * fb[1];
-            ebL += Hb;
-            pbL += Hb * irhoL;
-            irhobL += Hb * dL.p;
-            ebR += Hb;
-            pbR += Hb * irhoR;
-            irhobR += Hb * dR.p;
+            eb += Hb;
+            pb += Hb * irho;
+            irhob += Hb * dd.p;
 #pragma unroll
-            for (int n = 0; n < DIM; n++) {
-                velbL[n] += Hb * velL[n] + 0.5 * mA * fb[2 + n];
-                velbR[n] += Hb * velR[n] + 0.5 * mA * fb[2 + n];
-            }
+            for (int n = 0; n < DIM; n++) velb[n] += Hb * vel[n] + 0.5 * mA * fb[2 + n];
         }
     }
     if (NS > 0 && spadv) {
-        // LEFT upwinds the left state, anything else the right one
-        const bool left = dir == ABL_DIR_LEFT;
-        const double* u = left ? uL : uR;
-        const double irho = left ? irhoL : irhoR;
-        double* ub = left ? ubL : ubR;
-        double irb = 0;
 #pragma unroll
         for (int s = 0; s < NS; s++) {
-            mfb += areaMag * u[D::NE + s] * irho * fb[D::NE + s];
-            const double Yb = mA * fb[D::NE + s];
-            ub[D::NE + s] += Yb * irho;
-            irb += Yb * u[D::NE + s];
+            const double Y = u[D::NE + s] * irho;
+            const double Y_o = xch(mask, Y);
+            mfb += areaMag * (upme ? Y : Y_o) * fb[D::NE + s];
+            if (upme) {
+                const double Yb = mA * fb[D::NE + s];
+                ub[D::NE + s] += Yb * irho;
+                irhob += Yb * u[D::NE + s];
+            }
         }
-        if (left)
-            irhobL += irb;
-        else
-            irhobR += irb;
     }
     double g[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (mfb != 0.0 || p12b != 0.0) {
-        const double x[8] = {unL, dL.a, rhoL, dL.p, unR, dR.a, rhoR, dR.p};
-        calc_vjp<FK>(P, x, mfb, p12b, g, rok);
-    }
-    ubL[0] += g[2];
-    ubR[0] += g[6];
+    if (mfb != 0.0 || p12b != 0.0) calc_vjp<FK>(P, x, mfb, p12b, g, rok);
+    const double gu = side ? g[4] : g[0], ga = side ? g[5] : g[1], gr = side ? g[6] : g[2], gp = side ? g[7] : g[3];
+    ub[0] += gr;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-        velbL[d] += g[0] * norm[d];
-        velbR[d] += g[4] * norm[d];
-        ubL[2 + d] += velbL[d] * irhoL;
-        irhobL += velbL[d] * uL[2 + d];
-        ubR[2 + d] += velbR[d] * irhoR;
-        irhobR += velbR[d] * uR[2 + d];
+        velb[d] += gu * norm[d];
+        ub[2 + d] += velb[d] * irho;
+        irhob += velb[d] * u[2 + d];
     }
-    ubL[0] -= irhobL * irhoL * irhoL;
-    ubR[0] -= irhobR * irhoR * irhoR;
-    decode_vjp<DIM, NS>(P, NS, uL, dL, ebL, g[1], pbL + g[3], ubL);
-    decode_vjp<DIM, NS>(P, NS, uR, dR, ebR, g[5], pbR + g[7], ubR);
+    ub[0] -= irhob * irho * irho;
+    decode_vjp<DIM, NS>(P, NS, u, dd, eb, ga, pb + gp, ub);
 }
 
-// diffusion (NavierStokesTransport::DiffusionFlux, SpeciesTransport diffusion) backwards: the face
-// state/aux are averages of the two cells and the face gradient the average of their aux gradients,
-// so each side receives half of fsb, fab, gfb
+// diffusion (NavierStokesTransport::DiffusionFlux, SpeciesTransport diffusion) backwards. fs, fa and
+// gf are the face state, aux and aux gradient (averages of the two cells); each side receives half of
+// the returned fsb, fab, gfb.
 template <int DIM, int NS>
-__device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* normal, const double* cL, const double* cR, const double* aL,
-                                              const double* aR, const double* gL, const double* gR, bool dif, bool spdif, const double* fb,
-                                              double* fsb, double* fab, double* gfb) {
+__device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* normal, const double* fs, const double* fa, const double* gf, bool dif,
+                                              bool spdif, const double* fb, double* fsb, double* fab, double* gfb) {
     using D = Dims<DIM, NS>;
-    double fs[D::NC], fa[D::NA];
 #pragma unroll
-    for (int k = 0; k < D::NC; k++) {
-        fs[k] = cL[k] * 0.5 + cR[k] * 0.5;
-        fsb[k] = 0.0;
-    }
+    for (int k = 0; k < D::NC; k++) fsb[k] = 0.0;
 #pragma unroll
-    for (int k = 0; k < D::NA; k++) {
-        fa[k] = aL[k] * 0.5 + aR[k] * 0.5;
-        fab[k] = 0.0;
-    }
+    for (int k = 0; k < D::NA; k++) fab[k] = 0.0;
 #pragma unroll
     for (int k = 0; k < D::NA * DIM; k++) gfb[k] = 0.0;
     double mu, kc, diff;
     transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
     double mub = 0, kb = 0, Db = 0;
     if (dif) {
-        double gv[DIM * DIM], gT[DIM];
-#pragma unroll
-        for (int i = 0; i < DIM * DIM; i++) gv[i] = 0.5 * gL[DIM + i] + 0.5 * gR[DIM + i];
-#pragma unroll
-        for (int d = 0; d < DIM; d++) gT[d] = 0.5 * gL[d] + 0.5 * gR[d];
+        const double* gT = gf;
+        const double* gv = gf + DIM;
         double divVel = 0;
 #pragma unroll
         for (int c = 0; c < DIM; ++c) divVel += gv[c * DIM + c];
@@ -617,28 +582,24 @@ __device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* norma
             kb -= normal[d] * gT[d] * fb[1];
             gfb[d] -= normal[d] * kc * fb[1];
         }
-        double gvb[DIM * DIM], divb = 0;
-#pragma unroll
-        for (int i = 0; i < DIM * DIM; i++) gvb[i] = 0.0;
+        double divb = 0;
 #pragma unroll
         for (int c = 0; c < DIM; ++c)
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
                 const double tb = taub[c * DIM + d];
                 if (c == d) {
-                    gvb[c * DIM + c] += 2.0 * mu * tb;
+                    gfb[DIM + c * DIM + c] += 2.0 * mu * tb;
                     divb -= 2.0 * mu / 3.0 * tb;
                     mub += 2.0 * tb * (gv[c * DIM + c] - divVel / 3.0);
                 } else {
-                    gvb[c * DIM + d] += mu * tb;
-                    gvb[d * DIM + c] += mu * tb;
+                    gfb[DIM + c * DIM + d] += mu * tb;
+                    gfb[DIM + d * DIM + c] += mu * tb;
                     mub += tb * (gv[c * DIM + d] + gv[d * DIM + c]);
                 }
             }
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) gvb[c * DIM + c] += divb;
-#pragma unroll
-        for (int i = 0; i < DIM * DIM; i++) gfb[DIM + i] += gvb[i];
+        for (int c = 0; c < DIM; ++c) gfb[DIM + c * DIM + c] += divb;
     }
     if constexpr (NS > 0) {
         if (spdif) {
@@ -651,7 +612,7 @@ __device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* norma
                 double hsb = 0;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
-                    const double gy = 0.5 * gL[yoff + s * DIM + d] + 0.5 * gR[yoff + s * DIM + d];
+                    const double gy = gf[yoff + s * DIM + d];
                     const double q = -normal[d] * (fb[D::NE + s] + hs * fb[1]);
                     rhob += q * diff * gy;
                     Db += q * density * gy;
@@ -676,96 +637,84 @@ struct AdjRow {
     static constexpr int N = GA + D::NA * DIM;
 };
 
-// one face backwards: the adjoint contributions are added into each side's accumulator row (dst[0]
-// left, dst[1] right; nullptr drops a side that another tile accumulates)
+// one face backwards, this lane's side: the adjoint contributions are added into the side's
+// accumulator row dst (nullptr drops a side that another tile accumulates)
 template <int DIM, int NS, int FK>
-__device__ __forceinline__ void face_vjp(const DevMesh& M, const Phys& P, int L, int R, const double* normal, const double* fdx,
-                                         const double* __restrict__ U, const double* __restrict__ aux, const double* __restrict__ grad,
-                                         const double* __restrict__ agrad, const double* __restrict__ Fb, double* dstL, double* dstR,
-                                         bool* ok, bool* rok) {
+__device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, unsigned mask, int side, int me, const double* normal,
+                                              const double* fdxo, const double* __restrict__ U, const double* __restrict__ aux,
+                                              const double* __restrict__ grad, const double* __restrict__ agrad, const double* __restrict__ Fb,
+                                              double* dst, bool* ok, bool* rok) {
     using D = Dims<DIM, NS>;
     using GR = GradRows<DIM, NS, double>;
     using AR = AdjRow<DIM, NS>;
-    // dF_L/dflux = -1/V_L, dF_R/dflux = +1/V_R on owned cells
+    // dF_L/dflux = -1/V_L, dF_R/dflux = +1/V_R on owned cells; fb = (right term) + (left term)
+    const bool own = M.kind[me] == ABL_CELL_OWNED;
+    const double iv = own ? M.ivol[me] : 0.0;
     double fb[D::NC];
-    const bool oL = M.kind[L] == ABL_CELL_OWNED, oR = M.kind[R] == ABL_CELL_OWNED;
-    const double ivL = oL ? M.ivol[L] : 0.0, ivR = oR ? M.ivol[R] : 0.0;
 #pragma unroll
-    for (int k = 0; k < D::NC; k++)
-        fb[k] = (oR ? __ldg(Fb + (size_t)R * D::NC + k) * ivR : 0.0) - (oL ? __ldg(Fb + (size_t)L * D::NC + k) * ivL : 0.0);
-    double cL[D::NC], cR[D::NC];
-    load_state<DIM, NS>(U, L, cL);
-    load_state<DIM, NS>(U, R, cR);
+    for (int k = 0; k < D::NC; k++) {
+        const double t = own ? __ldg(Fb + (size_t)me * D::NC + k) * iv : 0.0;
+        const double mine = side ? t : -t;
+        fb[k] = mine + xch(mask, mine);
+    }
+    double c[D::NC];
+    load_state<DIM, NS>(U, me, c);
     const bool adv = P.advection && P.flux != ABL_FLUX_OFF;
     const bool spadv = NS > 0 && P.sp_adv && P.flux != ABL_FLUX_OFF;
     if (adv || spadv) {
         const bool lsq = P.recon == ABL_RECON_LEASTSQUARES;
-        double uL[D::NC], uR[D::NC];
+        double u[D::NC];
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
-            uL[k] = cL[k];
-            uR[k] = cR[k];
+            double dot = 0;
+            if (lsq) {
+#pragma unroll
+                for (int d = 0; d < DIM; d++) dot += __ldg(grad + (size_t)me * GR::GS + k * DIM + d) * fdxo[d];
+            }
+            u[k] = lsq ? c[k] + dot : c[k];
         }
-        if (lsq) {
+        double guess = 300.0;
+        if (NS > 0 && P.eos == ABL_EOS_NASA7) {
+            const double Tme = __ldg(aux + (size_t)me * D::NA), To = xch(mask, Tme);
+            const double TL = side ? To : Tme, TR = side ? Tme : To;
+            guess = side ? TL * .33 + .67 * TR : TL * .67 + .33 * TR;
+        }
+        double ub[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) ub[k] = 0.0;
+        advection_vjp_side<DIM, NS, FK>(P, mask, side, normal, u, guess, adv, spadv, fb, ub, ok, rok);
+        // u_face = u_cell + g . dx: the identity part to the state, the outer product with dx to the gradient
+        if (dst) {
 #pragma unroll
             for (int k = 0; k < D::NC; k++) {
-                double gl[DIM], gr[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) {
-                    gl[d] = __ldg(grad + (size_t)L * GR::GS + k * DIM + d);
-                    gr[d] = __ldg(grad + (size_t)R * GR::GS + k * DIM + d);
-                }
-                double dotL = 0, dotR = 0;
-#pragma unroll
-                for (int d = 0; d < DIM; d++) {
-                    dotL += gl[d] * fdx[d];
-                    dotR += gr[d] * fdx[3 + d];
-                }
-                uL[k] = uL[k] + dotL;
-                uR[k] = uR[k] + dotR;
-            }
-        }
-        double TL = 300.0, TR = 300.0;
-        if (NS > 0 && P.eos == ABL_EOS_NASA7) {
-            TL = __ldg(aux + (size_t)L * D::NA);
-            TR = __ldg(aux + (size_t)R * D::NA);
-        }
-        double ubL[D::NC], ubR[D::NC];
-#pragma unroll
-        for (int k = 0; k < D::NC; k++) ubL[k] = ubR[k] = 0.0;
-        advection_vjp<DIM, NS, FK>(P, normal, uL, uR, TL, TR, adv, spadv, fb, ubL, ubR, ok, rok);
-        // u_face = u_cell + g . dx: the identity part to the state, the outer product with dx to the gradient
-#pragma unroll
-        for (int k = 0; k < D::NC; k++) {
-            if (dstL) {
-                dstL[AR::U + k] += ubL[k];
+                dst[AR::U + k] += ub[k];
                 if (lsq)
 #pragma unroll
-                    for (int d = 0; d < DIM; d++) dstL[AR::G + k * DIM + d] += ubL[k] * fdx[d];
-            }
-            if (dstR) {
-                dstR[AR::U + k] += ubR[k];
-                if (lsq)
-#pragma unroll
-                    for (int d = 0; d < DIM; d++) dstR[AR::G + k * DIM + d] += ubR[k] * fdx[3 + d];
+                    for (int d = 0; d < DIM; d++) dst[AR::G + k * DIM + d] += ub[k] * fdxo[d];
             }
         }
     }
     const bool dif = P.diffusion && P.transport != ABL_TRANSPORT_NONE;
     const bool spdif = NS > 0 && P.sp_dif && P.transport != ABL_TRANSPORT_NONE;
     if (dif || spdif) {
-        double aL[D::NA], aR[D::NA];
-        cell_aux<DIM, NS>(P, cL, aux, L, aL);
-        cell_aux<DIM, NS>(P, cR, aux, R, aR);
-        double gL[D::NA * DIM], gR[D::NA * DIM];
-        load_row<D::NA * DIM, double>(agrad + (size_t)L * GR::AS, gL);
-        load_row<D::NA * DIM, double>(agrad + (size_t)R * GR::AS, gR);
-        double fsb[D::NC], fab[D::NA], gfb[D::NA * DIM];
-        diffusion_vjp<DIM, NS>(P, normal, cL, cR, aL, aR, gL, gR, dif, spdif, fb, fsb, fab, gfb);
+        // face averages: a + b is commutative, so both lanes hold identical values
+        double fs[D::NC], fa[D::NA], gf[D::NA * DIM];
+        {
+            double a[D::NA];
+            cell_aux<DIM, NS>(P, c, aux, me, a);
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
-            double* dst = s == 0 ? dstL : dstR;
-            if (!dst) continue;
+            for (int k = 0; k < D::NA; k++) fa[k] = a[k] * 0.5 + xch(mask, a[k]) * 0.5;
+        }
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) fs[k] = c[k] * 0.5 + xch(mask, c[k]) * 0.5;
+#pragma unroll
+        for (int k = 0; k < D::NA * DIM; k++) {
+            const double gm = __ldg(agrad + (size_t)me * GR::AS + k);
+            gf[k] = 0.5 * gm + 0.5 * xch(mask, gm);
+        }
+        double fsb[D::NC], fab[D::NA], gfb[D::NA * DIM];
+        diffusion_vjp<DIM, NS>(P, normal, fs, fa, gf, dif, spdif, fb, fsb, fab, gfb);
+        if (dst) {
 #pragma unroll
             for (int k = 0; k < D::NC; k++) dst[AR::U + k] += 0.5 * fsb[k];
 #pragma unroll
@@ -789,90 +738,21 @@ struct AdjOut {
     double* ab;     // [nc][NA] aux adjoint, own terms
 };
 
-template <int DIM, int NS, int LIM>
-__device__ __forceinline__ void limit_field_vjp(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U, const double* uc,
-                                                const double* g, const double* gtb, double* gbar, double* ub, double* beta, int* fstar, int k0,
-                                                int k1) {
-    using D = Dims<DIM, NS>;
-    double phi[D::NC];
-    int ist[D::NC];
-#pragma unroll
-    for (int k = 0; k < D::NC; k++) {
-        phi[k] = DBL_MAX;
-        ist[k] = -1;
-    }
-#pragma unroll 1
-    for (int i = beg; i < end; i++) {
-        const int2 ce = M.cone[i];
-        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
-        double v[DIM];
-#pragma unroll
-        for (int d = 0; d < DIM; d++) v[d] = __ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d);
-        double un[D::NC];
-        load_state<DIM, NS>(U, n, un);
-#pragma unroll
-        for (int k = 0; k < D::NC; k++) {
-            if (k < k0 || k >= k1) continue;
-            double denom = 0;
-#pragma unroll
-            for (int d = 0; d < DIM; d++) denom += g[k * DIM + d] * v[d];
-            const double flim = 0.5 * (un[k] - uc[k]) * rcp64(denom);
-            const double l = limiter_k<LIM, double>(P.limiter, flim);
-            if (!(phi[k] < l)) {  // pmin(phi, l) takes l
-                phi[k] = l;
-                ist[k] = i;
-            }
-        }
-    }
-    bool cancel = false;
-#pragma unroll
-    for (int k = 0; k < D::NC; k++) {
-        if (k < k0 || k >= k1) continue;
-        if (phi[k] == 0.0)
-#pragma unroll
-            for (int d = 0; d < DIM; d++)
-                if (fabs(g[k * DIM + d]) > P.max_lim_grad) cancel = true;
-    }
-#pragma unroll
-    for (int k = 0; k < D::NC; k++) {
-        if (k < k0 || k >= k1) continue;
-        double phib = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-            gbar[k * DIM + d] = cancel ? 0.0 : phi[k] * gtb[k * DIM + d];
-            phib += gtb[k * DIM + d] * g[k * DIM + d];
-        }
-        if (cancel || ist[k] < 0 || phib == 0.0) continue;
-        const int2 ce = M.cone[ist[k]];
-        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
-        double v[DIM], denom = 0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-            v[d] = __ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d);
-            denom += g[k * DIM + d] * v[d];
-        }
-        const double idn = rcp64(denom);
-        const double r = 0.5 * (__ldg(U + (size_t)n * D::NC + k) - uc[k]) * idn;
-        const double dl = limiter_k<LIM, Dual>(P.limiter, Dual(r, 1.0)).d;
-        const double rb = dl * phib;
-        if (rb == 0.0 || !isfinite(rb) || !isfinite(r)) continue;
-        const double bk = 0.5 * rb * idn;  // d r / d (u_n - u_c) = 1 / (2 denom)
-        beta[k] = bk;
-        fstar[k] = f;
-        ub[k] -= bk;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) gbar[k * DIM + d] -= r * rb * idn * v[d];  // d r / d denom = -r / denom
-    }
-}
+// forward records of k_gradient<..., REC = true>: unlimited gradient, applied limiter factor, and the
+// cone entry of the minimising face per component
+struct GradRec {
+    const double* graw;
+    const double* phi;
+    const int* ist;
+};
 
 template <int DIM, int NS, int LIM>
 __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c, const double* __restrict__ U, const double* acc,
-                                         const AdjOut<DIM, NS>& out, bool do_state, bool do_aux) {
+                                         const GradRec& rec, const AdjOut<DIM, NS>& out, bool do_state, bool do_aux) {
     using D = Dims<DIM, NS>;
     using GR = GradRows<DIM, NS, double>;
     using AR = AdjRow<DIM, NS>;
     const uint8_t kind = M.kind[c];
-    const int beg = M.cone_ptr[c], end = M.cone_ptr[c + 1];
     double ub[D::NC], gbar[D::NC * DIM], beta[D::NC];
     int fst[D::NC];
 #pragma unroll
@@ -884,43 +764,48 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
 #pragma unroll
     for (int k = 0; k < D::NC * DIM; k++) gbar[k] = 0.0;
     if (do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO)) {
-        double uc[D::NC], g[D::NC * DIM], ws[DIM];
-        load_state<DIM, NS>(U, c, uc);
+        // g~ = phi g (0 when cancelled): g-bar = phi g~-bar, plus the limiter's own dependence on g and on
+        // the minimising neighbour through r = (u_n - u_c) / (2 g . dx)
+        const double* g = rec.graw + (size_t)c * GR::GS;
 #pragma unroll
-        for (int k = 0; k < D::NC * DIM; k++) g[k] = 0.0;
-#pragma unroll
-        for (int d = 0; d < DIM; d++) ws[d] = 0.0;
-#pragma unroll 1
-        for (int i = beg; i < end; i++) {
-            const int2 ce = M.cone[i];
-            if (ce.y & kConeBoundary) continue;
-            const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
-            double w[DIM], un[D::NC];
+        for (int k = 0; k < D::NC; k++) {
+            const double ph = __ldg(rec.phi + (size_t)c * D::NC + k);
+            const int i = __ldg(rec.ist + (size_t)c * D::NC + k);
+            double phib = 0;
 #pragma unroll
             for (int d = 0; d < DIM; d++) {
-                w[d] = __ldg(M.cgrad + 6 * (size_t)f + 3 * sc + d);
-                ws[d] += w[d];
+                const double gt = acc[AR::G + k * DIM + d];
+                gbar[k * DIM + d] = ph * gt;
+                phib += gt * __ldg(g + k * DIM + d);
             }
-            load_state<DIM, NS>(U, n, un);
+            if (i < 0 || phib == 0.0) continue;
+            const int2 ce = M.cone[i];
+            const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+            double v[DIM], denom = 0;
 #pragma unroll
-            for (int k = 0; k < D::NC; k++) {
-                const double delta = un[k] - uc[k];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) g[k * DIM + d] += w[d] * delta;
+            for (int d = 0; d < DIM; d++) {
+                v[d] = __ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d);
+                denom += __ldg(g + k * DIM + d) * v[d];
             }
+            const double idn = rcp64(denom);
+            const double r = 0.5 * (__ldg(U + (size_t)n * D::NC + k) - __ldg(U + (size_t)c * D::NC + k)) * idn;
+            const double dl = limiter_k<LIM, Dual>(P.limiter, Dual(r, 1.0)).d;
+            const double rb = dl * phib;
+            if (rb == 0.0 || !isfinite(rb) || !isfinite(r)) continue;
+            const double bk = 0.5 * rb * idn;  // d r / d (u_n - u_c) = 1 / (2 denom)
+            beta[k] = bk;
+            fst[k] = f;
+            ub[k] -= bk;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) gbar[k * DIM + d] -= r * rb * idn * v[d];  // d r / d denom = -r / denom
         }
-        if (P.limiter != ABL_LIMITER_NONE) {
-            limit_field_vjp<DIM, NS, LIM>(M, P, beg, end, U, uc, g, acc + AR::G, gbar, ub, beta, fst, 0, D::NE);
-            if (NS > 0) limit_field_vjp<DIM, NS, LIM>(M, P, beg, end, U, uc, g, acc + AR::G, gbar, ub, beta, fst, D::NE, D::NC);
-        } else {
+        // g = sum_f w_f (u_n - u_c): the own-cell term, with the cell's summed weights
 #pragma unroll
-            for (int k = 0; k < D::NC * DIM; k++) gbar[k] = acc[AR::G + k];
+        for (int d = 0; d < DIM; d++) {
+            const double ws = __ldg(M.wsum + 6 * (size_t)c + d);
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) ub[k] -= ws * gbar[k * DIM + d];
         }
-        // g = sum_f w_f (u_n - u_c): the own-cell term
-#pragma unroll
-        for (int k = 0; k < D::NC; k++)
-#pragma unroll
-            for (int d = 0; d < DIM; d++) ub[k] -= ws[d] * gbar[k * DIM + d];
     }
     double ab[D::NA], gab[D::NA * DIM];
 #pragma unroll
@@ -929,20 +814,12 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
 #pragma unroll
     for (int k = 0; k < D::NA * DIM; k++) gab[k] = auxg ? acc[AR::GA + k] : 0.0;
     if (auxg) {
-        double ws[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; d++) ws[d] = 0.0;
-#pragma unroll 1
-        for (int i = beg; i < end; i++) {
-            const int2 ce = M.cone[i];
-            const int f = ce.x, sc = (ce.y & kConeSide) ? 1 : 0;
+        for (int d = 0; d < DIM; d++) {
+            const double ws = __ldg(M.wsum + 6 * (size_t)c + 3 + d);
 #pragma unroll
-            for (int d = 0; d < DIM; d++) ws[d] += __ldg(M.fgrad + 6 * (size_t)f + 3 * sc + d);
+            for (int k = 0; k < D::NA; k++) ab[k] -= ws * gab[k * DIM + d];
         }
-#pragma unroll
-        for (int k = 0; k < D::NA; k++)
-#pragma unroll
-            for (int d = 0; d < DIM; d++) ab[k] -= ws[d] * gab[k * DIM + d];
     }
     if (out.gb) {
         double* o = out.gb + (size_t)c * GR::GS;
@@ -967,18 +844,19 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
 // ---------------------------------------------------------------------------------------------------
 // kernels
 // ---------------------------------------------------------------------------------------------------
-// resident CTAs per SM the register budget targets (shared memory holds 3 tiles of accumulators at
-// 0 species; the species instances need more of both)
+// resident CTAs per SM the register budget targets (shared memory holds 2 tiles of accumulators at
+// 0 species; one at the species counts)
 template <int NS>
 struct AdjBlocks {
-    static constexpr int tile = NS == 0 ? 3 : 2;
+    static constexpr int tile = NS == 0 ? 2 : 1;
 };
 
+// 256 threads: two lanes per face, one colour (at most 128 faces) per pass
 template <int DIM, int NS, int FK, int LIM>
-__global__ void __launch_bounds__(128, AdjBlocks<NS>::tile) k_tile_adjoint(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
-                                                         const double* __restrict__ grad, const double* __restrict__ agrad,
-                                                         const double* __restrict__ Fb, AdjOut<DIM, NS> out, double* __restrict__ nbrec,
-                                                         int do_state, int do_aux, int* status) {
+__global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ aux,
+                                                                          const double* __restrict__ grad, const double* __restrict__ agrad,
+                                                                          const double* __restrict__ Fb, GradRec rec, AdjOut<DIM, NS> out,
+                                                                          double* __restrict__ nbrec, int do_state, int do_aux, int* status) {
     using AR = AdjRow<DIM, NS>;
     extern __shared__ double sacc[];  // [tile cells][AR::N]
     const int t = blockIdx.x;
@@ -986,42 +864,42 @@ __global__ void __launch_bounds__(128, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
     for (int i = threadIdx.x; i < nct * AR::N; i += blockDim.x) sacc[i] = 0.0;
     __syncthreads();
     bool ok = true, rok = true;
+    const int side = threadIdx.x & 1, pair = threadIdx.x >> 1;
     const int base = M.col_base[t], ncol = M.col_base[t + 1] - base - 1;
     for (int q = 0; q < ncol; q++) {
-        const int fe = M.col_start[base + q + 1];
-        for (int i = M.col_start[base + q] + threadIdx.x; i < fe; i += blockDim.x) {  // one pass: a colour has <= 128 faces
+        const int i = M.col_start[base + q] + pair;
+        const bool act = i < M.col_start[base + q + 1];
+        const unsigned mask = __ballot_sync(0xffffffffu, act);  // both lanes of a face share act
+        if (act) {
             const int2 lr = M.tf_cells[i];
-            double normal[DIM], fdx[6];
+            const int me = side ? lr.y : lr.x;
+            double normal[DIM], fdxo[3];
 #pragma unroll
             for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_normal + 3 * (size_t)i + d);
 #pragma unroll
-            for (int d = 0; d < 6; d++) fdx[d] = __ldg(M.tf_fdx + 6 * (size_t)i + d);
-            // destination rows: this tile's accumulator, the record of a non-owned side, or none
+            for (int d = 0; d < 3; d++) fdxo[d] = __ldg(M.tf_fdx + 6 * (size_t)i + 3 * side + d);
+            // destination: this tile's accumulator, the record of a non-owned side, or none
             const uint32_t slots = M.tf_slot[i];
+            const int slot = side ? int(slots >> 16) : int(slots & 0xffff);
             const int nb = M.tf_nb[i];
-            double* dst[2];
-#pragma unroll
-            for (int s = 0; s < 2; s++) {
-                const int slot = s == 0 ? int(slots & 0xffff) : int(slots >> 16);
-                dst[s] = nullptr;
-                if (slot != 0xffff)
-                    dst[s] = sacc + (size_t)slot * AR::N;
-                else if (nb >= 0 && M.kind[s == 0 ? lr.x : lr.y] != ABL_CELL_OWNED)
-                    dst[s] = nbrec + (size_t)nb * AR::N;
-            }
-            face_vjp<DIM, NS, FK>(M, P, lr.x, lr.y, normal, fdx, U, aux, grad, agrad, Fb, dst[0], dst[1], &ok, &rok);
+            double* dst = nullptr;
+            if (slot != 0xffff)
+                dst = sacc + (size_t)slot * AR::N;
+            else if (nb >= 0 && M.kind[me] != ABL_CELL_OWNED)
+                dst = nbrec + (size_t)nb * AR::N;
+            face_vjp_side<DIM, NS, FK>(M, P, mask, side, me, normal, fdxo, U, aux, grad, agrad, Fb, dst, &ok, &rok);
         }
         __syncthreads();
     }
     for (int j = threadIdx.x; j < nct; j += blockDim.x)
-        cell_vjp<DIM, NS, LIM>(M, P, M.tile_cells[cb + j], U, sacc + (size_t)j * AR::N, out, do_state, do_aux);
+        cell_vjp<DIM, NS, LIM>(M, P, M.tile_cells[cb + j], U, sacc + (size_t)j * AR::N, rec, out, do_state, do_aux);
     if (!ok) atomicOr(status, kStatusEos);
     if (!rok) atomicOr(status, kStatusRiemann);
 }
 
 template <int DIM, int NS, int LIM>
 __global__ void __launch_bounds__(128) k_adjoint_nonowned(DevMesh M, Phys P, const double* __restrict__ U, const double* __restrict__ nbrec,
-                                                          AdjOut<DIM, NS> out, int do_state, int do_aux) {
+                                                          GradRec rec, AdjOut<DIM, NS> out, int do_state, int do_aux) {
     using AR = AdjRow<DIM, NS>;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= M.n_nonowned) return;
@@ -1036,7 +914,7 @@ __global__ void __launch_bounds__(128) k_adjoint_nonowned(DevMesh M, Phys P, con
 #pragma unroll
         for (int k = 0; k < AR::N; k++) acc[k] += r[k];
     }
-    cell_vjp<DIM, NS, LIM>(M, P, c, U, acc, out, do_state, do_aux);
+    cell_vjp<DIM, NS, LIM>(M, P, c, U, acc, rec, out, do_state, do_aux);
 }
 
 template <int DIM, int NS>

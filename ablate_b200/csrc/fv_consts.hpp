@@ -1,0 +1,10 @@
+// fv_consts.hpp -- constants shared by the host-side set-up and the device kernels.
+#pragma once
+
+namespace abl {
+
+// Faces per colour in a tile (the adjoint kernel runs one colour per pass, two lanes per face, on
+// 2 * kColorCap threads).
+constexpr int kColorCap = 128;
+
+}  // namespace abl

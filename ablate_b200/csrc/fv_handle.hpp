@@ -99,8 +99,9 @@ struct abl_fv {
     abl::DevBuf<float> grad32, agrad32;
     abl::DevBuf<int> status;
     // adjoint work buffers, allocated on the first VJP
-    abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb;
-    abl::DevBuf<int> adj_fstar;
+    abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb, adj_graw, adj_phi;
+    abl::DevBuf<int> adj_fstar, adj_ist;
+    abl::DevBuf<double> wsum;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;

@@ -19,6 +19,7 @@
 #include <cfloat>
 #include <type_traits>
 
+#include "fv_consts.hpp"
 #include "fv_physics.cuh"
 
 namespace abl {
@@ -54,6 +55,7 @@ struct DevMesh {
     const int* face_nb;
     int n_nonowned;
     const int* nonowned;  // cells that are not owned (boundary ghosts, halos)
+    const double* wsum;   // [nc][2][3] per cell: sum of its LSQ state weights (non-boundary faces), of its aux weights
 };
 
 template <int DIM, int NS>
@@ -210,14 +212,21 @@ __global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __
 // ---------------------------------------------------------------------------------------------------
 // limiter of one field (components k0..k1-1) of cell c with gradient g (DMPlexApplyLimiter_Internal,
 // cellInterpolant.cpp:282-328, and the cancel rule at :459-481)
-template <int DIM, int NS, class G, int LIM>
+// REC (the adjoint's forward pass) also records, per component, the applied factor (0 when the
+// gradient was cancelled) and the cone entry of the minimising face (-1: none, or cancelled).
+template <int DIM, int NS, class G, int LIM, bool REC = false>
 __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U,
-                                            const double* __restrict__ dU, const StateOf<G>* uc, G* g, int k0, int k1) {
+                                            const double* __restrict__ dU, const StateOf<G>* uc, G* g, int k0, int k1,
+                                            double* rphi = nullptr, int* rist = nullptr) {
     using D = Dims<DIM, NS>;
     using S = StateOf<G>;
     G phi[D::NC];
+    int ist[D::NC];
 #pragma unroll
-    for (int k = 0; k < D::NC; k++) phi[k] = big_value<G>();
+    for (int k = 0; k < D::NC; k++) {
+        phi[k] = big_value<G>();
+        ist[k] = -1;
+    }
 #pragma unroll 2
     for (int i = beg; i < end; i++) {
         const int2 ce = M.cone[i];
@@ -236,7 +245,15 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
             for (int d = 0; d < DIM; d++) denom += g[k * DIM + d] * v[d];
             const G diff = G(un[k] - uc[k]);
             const G flim = G(0.5) * diff * rcp64(denom);
-            phi[k] = pmin(phi[k], limiter_k<LIM, G>(P.limiter, flim));
+            if constexpr (REC) {
+                const G l = limiter_k<LIM, G>(P.limiter, flim);
+                if (!(phi[k] < l)) {  // pmin(phi, l) takes l
+                    phi[k] = l;
+                    ist[k] = i;
+                }
+            } else {
+                phi[k] = pmin(phi[k], limiter_k<LIM, G>(P.limiter, flim));
+            }
         }
     }
     bool cancel = false;
@@ -252,6 +269,10 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
 #pragma unroll
     for (int k = 0; k < D::NC; k++) {
         if (k < k0 || k >= k1) continue;
+        if constexpr (REC) {
+            rphi[k] = cancel ? 0.0 : double(phi[k]);
+            rist[k] = cancel ? -1 : ist[k];
+        }
 #pragma unroll
         for (int d = 0; d < DIM; d++) g[k * DIM + d] *= cancel ? G(0) : phi[k];
     }
@@ -261,10 +282,12 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
 // fields (non-boundary faces, cgrad weights) and of the aux fields (all faces, fgrad weights), a second
 // pass applies the limiter. Cells without a conserved-state gradient (boundary ghosts, outer halo) get
 // a zero row, so the flux kernel projects every cell without a branch.
-template <int DIM, int NS, class G, int LIM>
+template <int DIM, int NS, class G, int LIM, bool REC = false>
 __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMesh M, Phys P, const double* __restrict__ U,
                                                                     const double* __restrict__ dU, const double* __restrict__ aux,
-                                                                    G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux) {
+                                                                    G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux,
+                                                                    G* __restrict__ graw = nullptr, double* __restrict__ rphi = nullptr,
+                                                                    int* __restrict__ rist = nullptr) {
     using D = Dims<DIM, NS>;
     using GR = GradRows<DIM, NS, G>;
     using S = StateOf<G>;
@@ -315,7 +338,32 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 }
             }
         }
-        if (state && P.limiter != ABL_LIMITER_NONE) {
+        if constexpr (REC) {
+            // the unlimited gradient, and the limiter's factor and minimising face per component
+            double ph[D::NC];
+            int is[D::NC];
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) {
+                ph[k] = 1.0;
+                is[k] = -1;
+            }
+            if (do_state) {
+                G* o = graw + (size_t)c * GR::GS;
+#pragma unroll
+                for (int k = 0; k < D::NC * DIM; k++) o[k] = g[k];
+            }
+            if (state && P.limiter != ABL_LIMITER_NONE) {
+                limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, 0, D::NE, ph, is);
+                if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, ph, is);
+            }
+            if (do_state) {
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) {
+                    rphi[(size_t)c * D::NC + k] = ph[k];
+                    rist[(size_t)c * D::NC + k] = is[k];
+                }
+            }
+        } else if (state && P.limiter != ABL_LIMITER_NONE) {
             limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, 0, D::NE);
             if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC);
         }

@@ -102,12 +102,13 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
         k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, P, U, fv->aux.p, fv->status.p);
         check_launch();
     }
+    GradRec rec{fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p};
     if (fv->need_state_grad || fv->need_aux_grad) {
         mark(fv, "k_gradient", s);
-        if (P.limiter == ABL_LIMITER_MINMOD)
-            launch_gradient<DIM, NS, double, ABL_LIMITER_MINMOD>(fv, U, nullptr, fv->grad64.p, fv->agrad64.p, s);
-        else
-            launch_gradient<DIM, NS, double, -1>(fv, U, nullptr, fv->grad64.p, fv->agrad64.p, s);
+        auto kern = P.limiter == ABL_LIMITER_MINMOD ? k_gradient<DIM, NS, double, ABL_LIMITER_MINMOD, true> : k_gradient<DIM, NS, double, -1, true>;
+        kern<<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, nullptr, fv->aux.p, fv->grad64.p, fv->agrad64.p, fv->need_state_grad,
+                                                       fv->need_aux_grad, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p);
+        check_launch();
     }
     AdjOut<DIM, NS> out{fv->need_state_grad ? fv->adj_gb.p : nullptr, fv->adj_beta.p, fv->adj_fstar.p,
                         fv->need_aux_grad ? fv->adj_gab.p : nullptr, fv->adj_ub.p, fv->adj_ab.p};
@@ -125,12 +126,13 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
         else if (P.flux == ABL_FLUX_AUSM)
             kern = k_tile_adjoint<DIM, NS, ABL_FLUX_AUSM, -1>;
         ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        kern<<<M.n_tiles, 128, smem, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p, Fb, out, fv->adj_nb.p, ds, da, fv->status.p);
+        static_assert(2 * kColorCap == 256, "one colour per pass of the 256-thread adjoint CTA");
+        kern<<<M.n_tiles, 256, smem, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p, Fb, rec, out, fv->adj_nb.p, ds, da, fv->status.p);
         check_launch();
     }
     mark(fv, "k_adjoint_nonowned", s);
     if (M.n_nonowned > 0) {
-        k_adjoint_nonowned<DIM, NS, -1><<<blocks_for(M.n_nonowned, 128), 128, 0, s>>>(M, P, U, fv->adj_nb.p, out, ds, da);
+        k_adjoint_nonowned<DIM, NS, -1><<<blocks_for(M.n_nonowned, 128), 128, 0, s>>>(M, P, U, fv->adj_nb.p, rec, out, ds, da);
         check_launch();
     }
     mark(fv, "k_adjoint_gather", s);

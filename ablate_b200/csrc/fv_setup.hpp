@@ -9,6 +9,7 @@
 // The pseudo-inverse is computed by Householder QR of the offset matrix (full column rank) or by the
 // minimum-norm formula B^T (B B^T)^-1 (fewer offsets than dimensions: a boundary ghost cell).
 #pragma once
+#include "fv_consts.hpp"
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -136,8 +137,6 @@ struct Tiles {
     int n_nb = 0;                         // number of such records
     int max_colors = 0;
 };
-
-constexpr int kColorCap = 128;  // faces per colour = threads per CTA of the adjoint tile kernel
 
 inline uint64_t morton_spread(uint64_t x, int dim) {
     if (dim == 1) return x;
