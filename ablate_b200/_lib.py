@@ -87,6 +87,8 @@ SIGNATURES = {
     "abl_eos_batch": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, _dp, _dp, _dp]),
     "abl_eos_batch_noalloc": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),
+    "abl_rows_gather": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "abl_rows_scatter": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
 }
 
 

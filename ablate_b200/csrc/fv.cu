@@ -284,6 +284,22 @@ unsigned char* noalloc_scratch(int device) {
 }
 
 // =================================================================================================
+// halo pack (SCATTER = 0: dst[i] = src[idx[i]]) and unpack (SCATTER = 1: dst[idx[i]] = src[i]), one
+// thread per element so consecutive threads move consecutive doubles of a row
+template <int SCATTER>
+__global__ void __launch_bounds__(256) k_rows(const double* __restrict__ src, int width, const int32_t* __restrict__ idx, int64_t n,
+                                              double* __restrict__ dst) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * width) return;
+    const int64_t i = e / width;
+    const int k = (int)(e - i * width);
+    const int64_t r = __ldg(idx + i);
+    if (SCATTER)
+        dst[r * width + k] = src[i * width + k];
+    else
+        dst[i * width + k] = src[r * width + k];
+}
+
 extern "C" {
 
 const char* abl_last_error_string(void) { return g_last_error.c_str(); }
@@ -787,6 +803,26 @@ int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property
         ABL_CUDA(cudaMemcpyAsync(&bits, d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
         ABL_CUDA(cudaStreamSynchronize(s));
         if (bits & kStatusEos) throw AblError(ABL_ERR_EOS_NOT_CONVERGED, "temperature iteration did not converge");
+    });
+}
+
+int abl_rows_gather(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream) {
+    return guarded([&] {
+        if (n < 0 || width <= 0) throw std::invalid_argument("abl_rows_gather: bad size");
+        if (n == 0) return;
+        if (!src_dev || !idx_dev || !dst_dev) throw std::invalid_argument("abl_rows_gather: NULL argument");
+        k_rows<0><<<blocks_for(n * width, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(src_dev, width, idx_dev, n, dst_dev);
+        check_launch();
+    });
+}
+
+int abl_rows_scatter(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream) {
+    return guarded([&] {
+        if (n < 0 || width <= 0) throw std::invalid_argument("abl_rows_scatter: bad size");
+        if (n == 0) return;
+        if (!src_dev || !idx_dev || !dst_dev) throw std::invalid_argument("abl_rows_scatter: NULL argument");
+        k_rows<1><<<blocks_for(n * width, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(src_dev, width, idx_dev, n, dst_dev);
+        check_launch();
     });
 }
 

@@ -108,6 +108,18 @@ def tgv3d(n: int = 128, seed: int = 20261204, order: str = "morton") -> Workload
                     f"3D NS {n}^3 periodic hex, Taylor-Green M0.3 + 0.5% noise, AUSM+up + LSQ + minmod, mu 1.8e-5, Pr 0.72")
 
 
+def tgv3d_slab(n: int, nparts: int, rank: int, seed: int = 20261204, order: str = "morton"):
+    """Rank `rank`'s slab of the Taylor-Green case on an (n * nparts) x n x n periodic box, n^3 owned
+    cells per rank with a two-layer halo (weak scaling); returns (LocalDomain, Workload)."""
+    from .distributed import slab_domain
+    dom = slab_domain((n * nparts, n, n), nparts, rank, order=order)
+    w = tgv3d(2, seed)  # the physics of the case (its small mesh is replaced below)
+    U = tgv_state(dom.mesh, seed=seed + rank)
+    return dom, Workload("tgv3d", dom.mesh, w.eos, w.processes, w.petscfv_type, w.limiter, U,
+                         f"3D NS {n}^3 cells per GPU of a periodic {n * nparts}x{n}x{n} hex box cut in x-slabs, Taylor-Green M0.3 + 0.5% "
+                         "noise, AUSM+up + LSQ + minmod, mu 1.8e-5, Pr 0.72; 2-layer halo exchanged before every RHS")
+
+
 def synthetic_nasa7(ns: int, seed: int) -> list[dict]:
     """Seeded NASA-7 species with cp/R rising from [2.5, 4] at 300 K to at most 6 at 3000 K, one
     polynomial on both ranges (T_mid 1000 K), formation enthalpy h_f/R in [-3e4, 1e4] K and molar

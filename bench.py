@@ -7,9 +7,11 @@ minmod, constant viscosity), run at FP64 and on the mixed path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload tgv3d|sod2d|shear3d]
 
-With --gpus N > 1 it runs under torch.distributed.run, one rank per GPU, each rank holding its own
-copy of the workload (replicas; weak scaling, no data-path collective). Device times come from CUDA
-events around each RHS on the launching stream, L2 flushed between timed steps, max over ranks.
+With --gpus N > 1 it runs under torch.distributed.run, one rank per GPU: the Taylor-Green box is
+(128 N) x 128 x 128 cut into x-slabs, 128^3 owned cells per GPU (weak scaling), and every step is the
+two-layer halo exchange (pack kernel, NCCL point-to-point, unpack kernel) followed by the local RHS.
+Device times come from CUDA events around each step on the launching stream, L2 flushed between timed
+steps, max over ranks.
 ``--impl reference`` times the CPU restatement of the reference algorithm (the oracle; the reference
 itself needs PETSc/MPI/TChem, absent here) on all host cores, rank 0 only.
 """
@@ -60,10 +62,12 @@ def make_workload(name, n):
 
 def algorithmic_bytes(w):
     """Compulsory traffic of one RHS: read the FP64 state once, write the residual once, read 1/V per
-    cell; per face read two int32 cell indices and the FP64 area normal."""
+    owned cell; per face with an owned side read two int32 cell indices and the FP64 area normal."""
+    from ablate_b200 import _lib as L
     n_cells = int(w.mesh.n_interior)
     nc = w.U.shape[1]
-    n_faces = int(w.mesh.n_faces)
+    kind, fc = w.mesh.cell_kind, w.mesh.face_cells
+    n_faces = int(((kind[fc[:, 0]] == L.CELL_OWNED) | (kind[fc[:, 1]] == L.CELL_OWNED)).sum())
     return n_cells * (2 * nc * 8 + 8) + n_faces * (2 * 4 + w.mesh.dim * 8)
 
 
@@ -214,8 +218,18 @@ def main():
     from ablate_b200 import _lib as L
     from ablate_b200.workloads import initial_aux
 
-    w = make_workload(args.workload, args.n)
-    solver = w.solver(device=local)
+    drhs = None
+    if world > 1:
+        if args.workload != "tgv3d":
+            raise SystemExit("multi-GPU runs partition the tgv3d case")
+        from ablate_b200.distributed import DistributedRHS
+        from ablate_b200.workloads import tgv3d_slab
+        dom, w = tgv3d_slab(args.n or 128, world, rank)
+        drhs = DistributedRHS(dom, w.eos, w.processes, w.petscfv_type, w.limiter, device=local)
+        solver = drhs.solver
+    else:
+        w = make_workload(args.workload, args.n)
+        solver = w.solver(device=local)
     solver.SetAux(initial_aux(w))
     U = torch.from_numpy(w.U).to(dev)
     F = torch.zeros_like(U)
@@ -228,7 +242,10 @@ def main():
             dist.barrier()
 
     def rhs(prec):
-        solver.ComputeRHSDevice(0.0, U.data_ptr(), F.data_ptr(), prec, stream.cuda_stream)
+        if drhs is not None:
+            drhs.ComputeRHSDevice(0.0, U, F, prec)
+        else:
+            solver.ComputeRHSDevice(0.0, U.data_ptr(), F.data_ptr(), prec, stream.cuda_stream)
 
     results = {}
     kernels = {}
@@ -301,7 +318,7 @@ def main():
         return ms, split
 
     jvp_ms = vjp_ms = None
-    if L.PRECISION_FP64 in results:
+    if L.PRECISION_FP64 in results and world == 1:
         dU = torch.randn_like(U) * U.abs().mean(0, keepdim=True) * 1e-2
         dF = torch.zeros_like(U)
         jvp_ms, kernels["jvp"] = timed(lambda: solver.ComputeJVPDevice(0.0, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), 0, stream.cuda_stream), "JVP")
@@ -330,14 +347,26 @@ def main():
     Uh = torch.from_numpy(w.U).pin_memory()
     Fh = torch.zeros_like(Uh).pin_memory()
     Un, Fn = Uh.numpy(), Fh.numpy()
+
+    def e2e_step():
+        if drhs is not None:
+            # the rank's host state in, halo exchange + RHS, the residual out
+            U.copy_(Uh, non_blocking=True)
+            F.zero_()
+            drhs.ComputeRHSDevice(0.0, U, F, head)
+            Fh.copy_(F, non_blocking=True)
+            torch.cuda.current_stream(dev).synchronize()
+        else:
+            solver.ComputeRHSFunction(0.0, Un, Fn, head)
+
     for _ in range(2):
-        solver.ComputeRHSFunction(0.0, Un, Fn, head)
+        e2e_step()
     torch.cuda.synchronize(dev)
     barrier()
     e2e_steps = max(3, min(args.steps, 10))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        solver.ComputeRHSFunction(0.0, Un, Fn, head)
+        e2e_step()
     torch.cuda.synchronize(dev)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
     if world > 1:
@@ -361,8 +390,9 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if head == L.PRECISION_FP64 else "mixed f32/f64", "data": "synthetic",
-        "config": {"workload": w.name, "n_cells": n_cells, "n_faces": int(w.mesh.n_faces), "description": w.description,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "config": {"workload": w.name, "n_cells": world * n_cells, "cells_per_gpu": n_cells, "n_faces": int(w.mesh.n_faces), "description": w.description,
+                   "parallelism": (f"dp{world}: x-slab partition, 2-layer halo exchanged over NCCL point-to-point before every RHS "
+                                   f"({drhs.halo.bytes_per_exchange} B per rank per step)") if world > 1 else "single GPU",
                    "l2": "flushed (256 MiB write) between timed steps, outside the timed events"},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_achieved, "peak": peak, "unit": "GB/s", "frac": dom_achieved / peak,
                      "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed"),
@@ -378,9 +408,10 @@ def main():
         "vjp_over_rhs": (vjp_ms / results[L.PRECISION_FP64]) if vjp_ms else None,
         "vjp": {"ms_per_step": vjp_ms, "over_rhs_fp64": (vjp_ms / results[L.PRECISION_FP64]) if vjp_ms else None},
         "jvp": {"ms_per_step": jvp_ms, "over_rhs_fp64": (jvp_ms / results[L.PRECISION_FP64]) if jvp_ms else None},
-        "e2e": {"value": world * n_cells / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 2 * state_bytes,
-                "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,
-                "path": "abl_fv_rhs_host: pinned host U and F copied in, RHS, F copied out, every step"},
+        "e2e": {"value": world * n_cells / (e2e_ms * 1e-3) / 1e6, "unit": UNIT,
+                "h2d_bytes_per_step": (state_bytes if world > 1 else 2 * state_bytes), "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,
+                "path": ("per rank: pinned host U copied in, halo exchange + RHS, F copied out, every step" if world > 1 else
+                         "abl_fv_rhs_host: pinned host U and F copied in, RHS, F copied out, every step")},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -249,6 +249,15 @@ int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_
 int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved_dev,
                           const double* T_dev, double* out_dev, void* stream);
 
+/* Halo exchange between ranks of a partitioned mesh (the pack and unpack of DMGlobalToLocal's PetscSF
+ * broadcast of the state to ghost/overlap cells, src/solver/timeStepper.cpp:343-344). Row i of a
+ * width-column FP64 array is copied to or from a contiguous message buffer on `stream`:
+ *   gather:  dst[i][:] = src[idx[i]][:]   (pack the owned rows a neighbour needs)
+ *   scatter: dst[idx[i]][:] = src[i][:]   (unpack a neighbour's rows into the halo rows)
+ * All pointers are device pointers; the message travels between the calls (NCCL or peer copies). */
+int abl_rows_gather(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream);
+int abl_rows_scatter(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
