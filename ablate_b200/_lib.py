@@ -35,11 +35,18 @@ RECON_UPWIND, RECON_LEASTSQUARES = 0, 1
 LIMITER_NONE, LIMITER_ZERO, LIMITER_MINMOD, LIMITER_VANLEER, LIMITER_VANALBADA, LIMITER_SIN = range(6)
 CELL_OWNED, CELL_BOUNDARY, CELL_HALO, CELL_HALO_OUTER = range(4)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+BC_OUTFLOW, BC_DIRICHLET, BC_SLIP_WALL, BC_NOSLIP_WALL = range(4)
+BC_MAX_COMPONENTS = 16
+STEP_EULER, STEP_SSPRK3 = 0, 1
 RHS_OVERWRITE = 0x100
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 _u8p = C.POINTER(C.c_uint8)
+
+
+class BoundaryCondition(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("enforce_at_face", C.c_int32), ("value", C.c_double * BC_MAX_COMPONENTS)]
 
 
 class MeshDesc(C.Structure):
@@ -87,6 +94,13 @@ SIGNATURES = {
     "abl_eos_batch": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, _dp, _dp, _dp]),
     "abl_eos_batch_noalloc": (C.c_int, [C.POINTER(PhysicsDesc), C.c_int, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),
+    "abl_fv_set_boundary": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, _ip]),
+    "abl_fv_fill_ghosts": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+    "abl_fv_cfl_dt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.c_void_p]),
+    "abl_fv_normalize_species": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_rk_stage": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
+    "abl_fv_step": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_rows_gather": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
     "abl_rows_scatter": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
 }

@@ -13,6 +13,8 @@
 
 #include "fv_handle.hpp"
 #include "fv_setup.hpp"
+#include "fv_step.cuh"
+#include "fv_step.cuh"
 
 namespace abl {
 thread_local std::string g_last_error;
@@ -439,6 +441,39 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         }
         fv->status.alloc(1);
         fv->status.zero();
+        {
+            // boundary ghosts (one face each): interior neighbour and the unit normal out of the domain;
+            // per cell the smallest centroid-to-face-centroid distance (the CFL length)
+            std::vector<int32_t> gc, gn, gb;
+            std::vector<double> gnorm, rm(h.n_cells, 0.0);
+            for (int c = 0; c < h.n_cells; c++) {
+                double r = 1e300;
+                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                    const double* x = h.fdx.data() + 6 * (size_t)h.cone_face[i] + 3 * h.cone_side[i];
+                    r = std::min(r, std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]));
+                }
+                rm[c] = r;
+                if (h.kind[c] != ABL_CELL_BOUNDARY) continue;
+                const int i = h.cone_ptr[c], f = h.cone_face[i];
+                const double* n = mesh->face_normal + 3 * (size_t)f;
+                const double a = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+                const double sgn = h.cone_side[i] == 1 ? 1.0 : -1.0;  // the normal points left -> right
+                gc.push_back(c);
+                gn.push_back(h.cone_nbr[i]);
+                gb.push_back(0);
+                for (int d = 0; d < 3; d++) gnorm.push_back(d < h.dim ? sgn * n[d] / a : 0.0);
+            }
+            fv->n_ghost = (int)gc.size();
+            fv->ghost_cell.upload(gc.data(), gc.size());
+            fv->ghost_nbr.upload(gn.data(), gn.size());
+            fv->ghost_bc.upload(gb.data(), gb.size());
+            fv->ghost_normal.upload(gnorm.data(), gnorm.size());
+            fv->rmin.upload(rm.data(), rm.size());
+            abl_bc outflow{};
+            outflow.kind = ABL_BC_OUTFLOW;
+            fv->bc_table.upload(&outflow, 1);
+            fv->dt_bits.alloc(1);
+        }
 
         DevMesh& M = fv->mesh;
         M.dim = fv->dim;
@@ -803,6 +838,132 @@ int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property
         ABL_CUDA(cudaMemcpyAsync(&bits, d_status, sizeof(int), cudaMemcpyDeviceToHost, s));
         ABL_CUDA(cudaStreamSynchronize(s));
         if (bits & kStatusEos) throw AblError(ABL_ERR_EOS_NOT_CONVERGED, "temperature iteration did not converge");
+    });
+}
+
+int abl_fv_set_boundary(abl_fv* fv, int32_t n_bc, const abl_bc* table, const int32_t* cell_bc) {
+    return guarded([&] {
+        if (!fv || !table || n_bc < 1) throw std::invalid_argument("abl_fv_set_boundary: need a handle and at least one condition");
+        for (int b = 0; b < n_bc; b++)
+            if (table[b].kind < ABL_BC_OUTFLOW || table[b].kind > ABL_BC_NOSLIP_WALL)
+                throw std::invalid_argument("abl_fv_set_boundary: unknown condition kind in entry " + std::to_string(b));
+        ABL_CUDA(cudaSetDevice(fv->device));
+        std::vector<int32_t> gc(fv->n_ghost), gb(fv->n_ghost, 0);
+        if (fv->n_ghost) ABL_CUDA(cudaMemcpy(gc.data(), fv->ghost_cell.p, gc.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        if (cell_bc)
+            for (int j = 0; j < fv->n_ghost; j++) {
+                gb[j] = cell_bc[gc[j]];
+                if (gb[j] < 0 || gb[j] >= n_bc)
+                    throw std::invalid_argument("abl_fv_set_boundary: boundary cell " + std::to_string(gc[j]) + " names no condition");
+            }
+        fv->bc_table.upload(table, n_bc);
+        fv->ghost_bc.upload(gb.data(), gb.size());
+    });
+}
+
+}  // extern "C"
+
+namespace {
+GhostBC ghost_desc(abl_fv* fv) {
+    return GhostBC{fv->n_ghost, fv->ghost_cell.p, fv->ghost_nbr.p, fv->ghost_normal.p, fv->ghost_bc.p, fv->bc_table.p};
+}
+template <int DIM, int NS>
+void run_fill_ghosts(abl_fv* fv, double* U, cudaStream_t s) {
+    if (fv->n_ghost == 0) return;
+    k_fill_ghosts<DIM, NS><<<blocks_for(fv->n_ghost, 256), 256, 0, s>>>(ghost_desc(fv), U);
+    check_launch();
+}
+template <int DIM, int NS>
+void run_cfl_dt(abl_fv* fv, const double* U, double cfl, cudaStream_t s) {
+    const double big = DBL_MAX;
+    ABL_CUDA(cudaMemcpyAsync(fv->dt_bits.p, &big, sizeof(double), cudaMemcpyHostToDevice, s));
+    k_cfl_dt<DIM, NS><<<blocks_for(fv->n_cells, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->rmin.p, cfl, fv->dt_bits.p, fv->status.p);
+    check_launch();
+}
+template <int DIM, int NS>
+void run_normalize(abl_fv* fv, double* U, cudaStream_t s) {
+    if (NS == 0) return;
+    k_normalize_species<DIM, NS><<<blocks_for(fv->n_cells, 256), 256, 0, s>>>(fv->mesh, U);
+    check_launch();
+}
+void rk_stage(abl_fv* fv, double a, const double* U0, double b, const double* Us, double dt, const double* F, double* Uout, cudaStream_t s) {
+    k_rk_stage<><<<blocks_for((int64_t)fv->n_cells * fv->nc, 256), 256, 0, s>>>(fv->kind.p, fv->nc, fv->n_cells, a, U0, b, Us, dt, F, Uout);
+    check_launch();
+}
+}  // namespace
+
+extern "C" {
+
+int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream) {
+    (void)time;
+    return guarded([&] {
+        if (!fv || !U_dev) throw std::invalid_argument("abl_fv_fill_ghosts: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_cfl_dt(abl_fv* fv, const double* U_dev, double cfl, double* dt_host, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev || !dt_host) throw std::invalid_argument("abl_fv_cfl_dt: NULL argument");
+        if (!(cfl > 0)) throw std::invalid_argument("abl_fv_cfl_dt: cfl must be positive");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        ABL_DISPATCH(fv, run_cfl_dt, U_dev, cfl, s);
+        double dt = 0;
+        ABL_CUDA(cudaMemcpyAsync(&dt, fv->dt_bits.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        ABL_CUDA(cudaStreamSynchronize(s));
+        *dt_host = dt;
+    });
+}
+
+int abl_fv_normalize_species(abl_fv* fv, double* U_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev) throw std::invalid_argument("abl_fv_normalize_species: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_DISPATCH(fv, run_normalize, U_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const double* Us_dev, double dt, const double* F_dev, double* Uout_dev,
+                    void* stream) {
+    return guarded([&] {
+        if (!fv || !Us_dev || !F_dev || !Uout_dev || (a != 0.0 && !U0_dev)) throw std::invalid_argument("abl_fv_rk_stage: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        rk_stage(fv, a, U0_dev, b, Us_dev, dt, F_dev, Uout_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, int precision, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev) throw std::invalid_argument("abl_fv_step: NULL argument");
+        if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
+        if (scheme != ABL_STEP_EULER && scheme != ABL_STEP_SSPRK3) throw std::invalid_argument("abl_fv_step: unknown scheme");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->step_F.n != n) fv->step_F.alloc(n);
+        double* F = fv->step_F.p;
+        (void)time;
+        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+        dispatch_rhs(fv, U_dev, F, precision, 1, s);
+        if (scheme == ABL_STEP_EULER) {
+            rk_stage(fv, 0.0, nullptr, 1.0, U_dev, dt, F, U_dev, s);
+        } else {
+            // U1 = U + dt L(U); U1 = 3/4 U + 1/4 (U1 + dt L(U1)); U = 1/3 U + 2/3 (U1 + dt L(U1))
+            if (fv->step_U1.n != n) fv->step_U1.alloc(n);
+            double* U1 = fv->step_U1.p;
+            ABL_CUDA(cudaMemcpyAsync(U1, U_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            rk_stage(fv, 0.0, nullptr, 1.0, U_dev, dt, F, U1, s);
+            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            dispatch_rhs(fv, U1, F, precision, 1, s);
+            rk_stage(fv, 0.75, U_dev, 0.25, U1, dt, F, U1, s);
+            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            dispatch_rhs(fv, U1, F, precision, 1, s);
+            rk_stage(fv, 1.0 / 3.0, U_dev, 2.0 / 3.0, U1, dt, F, U_dev, s);
+        }
+        ABL_DISPATCH(fv, run_normalize, U_dev, s);
+        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
     });
 }
 

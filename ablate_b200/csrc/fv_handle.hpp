@@ -102,6 +102,13 @@ struct abl_fv {
     abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb, adj_graw, adj_phi;
     abl::DevBuf<int> adj_fstar, adj_ist;
     abl::DevBuf<double> wsum;
+    // boundary ghosts and time stepping
+    int n_ghost = 0;
+    abl::DevBuf<int> ghost_cell, ghost_nbr, ghost_bc;
+    abl::DevBuf<double> ghost_normal, rmin;
+    abl::DevBuf<abl_bc> bc_table;
+    abl::DevBuf<unsigned long long> dt_bits;
+    abl::DevBuf<double> step_U1, step_F;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;

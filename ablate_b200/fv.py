@@ -355,6 +355,60 @@ class FiniteVolumeSolver:
         L.check(L.lib.abl_fv_vjp(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(Fbar_ptr), C.c_void_p(Ubar_ptr), C.c_void_p(stream)),
                 "abl_fv_vjp")
 
+    # ---- the steps around the RHS (boundary ghosts, CFL step, explicit steps) ----------------------
+    def SetBoundary(self, table, cell_bc=None):
+        """Ghost-cell conditions: table = [(kind, value or None, enforce_at_face), ...] with kind one of
+        L.BC_*; cell_bc[c] = the entry of boundary ghost c (None: entry 0 for every ghost)."""
+        arr = (L.BoundaryCondition * len(table))()
+        for i, (kind, value, enforce) in enumerate(table):
+            arr[i].kind = int(kind)
+            arr[i].enforce_at_face = int(bool(enforce))
+            if value is not None:
+                for k, v in enumerate(value):
+                    arr[i].value[k] = float(v)
+        cb = None if cell_bc is None else np.ascontiguousarray(cell_bc, dtype=np.int32)
+        L.check(L.lib.abl_fv_set_boundary(self.handle, len(table), C.cast(arr, C.c_void_p), L.iptr(cb) if cb is not None else None),
+                "abl_fv_set_boundary")
+
+    def FillGhostsDevice(self, U_ptr: int, stream: int = 0):
+        L.check(L.lib.abl_fv_fill_ghosts(self.handle, 0.0, C.c_void_p(U_ptr), C.c_void_p(stream)), "abl_fv_fill_ghosts")
+
+    def CflTimeStepDevice(self, U_ptr: int, cfl: float, stream: int = 0) -> float:
+        dt = C.c_double(0.0)
+        L.check(L.lib.abl_fv_cfl_dt(self.handle, C.c_void_p(U_ptr), float(cfl), C.byref(dt), C.c_void_p(stream)), "abl_fv_cfl_dt")
+        return dt.value
+
+    def StepDevice(self, scheme: int, time: float, dt: float, U_ptr: int, precision: int = L.PRECISION_FP64, stream: int = 0):
+        L.check(L.lib.abl_fv_step(self.handle, scheme, time, dt, C.c_void_p(U_ptr), precision, C.c_void_p(stream)), "abl_fv_step")
+
+    def IntegrateDevice(self, U_ptr: int, t_end: float, cfl: float, scheme: int = L.STEP_EULER, precision: int = L.PRECISION_FP64,
+                        dt0: float = 0.1, stream: int = 0) -> int:
+        """March the device state to t_end as the reference's TimeStepper does with ts_adapt_type physics:
+        first step min(dt0, CFL step); after each step the next one is the CFL step of the state that step
+        started from (PETSc's adaptor runs before the solution takes the update), cut so the march ends
+        exactly at t_end without a sliver of a last step (TS_EXACTFINALTIME_MATCHSTEP, src/solver/
+        timeStepper.cpp:37; src/solver/adaptPhysics.cpp:3-24). Returns the number of steps."""
+        def match(h, t):
+            hmax = t_end - t
+            if t < t_end and t + h > t_end:
+                h = hmax
+            if t < t_end and t + h < t_end and h * 2.0 > hmax:
+                h = hmax / 2.0
+            if t < t_end and t + h < t_end and h * 1.01 > hmax:
+                h = hmax
+            return h
+
+        self.FillGhostsDevice(U_ptr, stream)
+        t, n = 0.0, 0
+        dt = match(min(dt0, self.CflTimeStepDevice(U_ptr, cfl, stream)), t)
+        while t < t_end:
+            nxt = self.CflTimeStepDevice(U_ptr, cfl, stream)
+            self.StepDevice(scheme, t, dt, U_ptr, precision, stream)
+            t = t_end if t + dt >= t_end or t_end - (t + dt) <= 1e-12 * t_end else t + dt
+            n += 1
+            dt = match(nxt, t)
+        return n
+
     def UpdateAux(self, locX: np.ndarray):
         """Recompute the aux fields (T, u, Y) from host state locX (CellSolver::UpdateAuxFields)."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

@@ -249,6 +249,54 @@ int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_
 int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved_dev,
                           const double* T_dev, double* out_dev, void* stream);
 
+/* ---- the steps around the RHS in a time step ------------------------------------------------------ */
+
+/* Ghost-cell boundary conditions (the Ghost / EssentialGhost update functions the reference applies
+ * through DMPlexInsertBoundaryValuesRiemann before every RHS: src/solver/solver.cpp:50-102,
+ * src/finiteVolume/boundaryConditions/ghost.cpp:17-28, essentialGhost.cpp:5-22). The reference takes an
+ * arbitrary host callback per boundary; on the device the common conditions are built in. */
+#define ABL_BC_OUTFLOW 0     /* ghost = interior (zero gradient)                                      */
+#define ABL_BC_DIRICHLET 1   /* ghost = value; with enforce_at_face, 2 value - interior (EssentialGhost) */
+#define ABL_BC_SLIP_WALL 2   /* ghost = interior with the normal momentum reversed                    */
+#define ABL_BC_NOSLIP_WALL 3 /* ghost = interior with the momentum reversed (zero velocity at the face)  */
+#define ABL_BC_MAX_COMPONENTS 16
+typedef struct abl_bc {
+    int32_t kind;
+    int32_t enforce_at_face;
+    double value[ABL_BC_MAX_COMPONENTS]; /* conserved state [rho, rhoE, rho u, rhoY] for ABL_BC_DIRICHLET */
+} abl_bc;
+
+/* Conditions table and, for every cell, the index of its condition (read for ABL_CELL_BOUNDARY cells
+ * only; cell_bc may be NULL: every ghost takes entry 0). Until the first call every ghost is outflow. */
+int abl_fv_set_boundary(abl_fv* fv, int32_t n_bc, const abl_bc* table, const int32_t* cell_bc);
+/* Fill the ghost rows of U_dev from their interior neighbours (before every RHS evaluation). */
+int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream);
+
+/* CFL time step of NavierStokesTransport::ComputeCflTimeStep (navierStokesTransport.cpp:209-278):
+ * min over owned cells of cfl * 2 r_min / (a / alpha + sum_d |u_d|), r_min the smallest cell-centroid to
+ * face-centroid distance, a the speed of sound at T(U) (guess 300 K), alpha the pressure-gradient
+ * scaling. Waits for `stream`; *dt_host receives this rank's minimum (reduce over ranks with MIN). */
+int abl_fv_cfl_dt(abl_fv* fv, const double* U_dev, double cfl, double* dt_host, void* stream);
+
+/* Mass-fraction clipping of SpeciesTransport::NormalizeSpecies (speciesTransport.cpp:343-403) on the
+ * owned rows; a no-op without species. */
+int abl_fv_normalize_species(abl_fv* fv, double* U_dev, void* stream);
+
+/* One stage of a Runge-Kutta step on the owned rows: Uout = a U0 + b (Us + dt F) (a == 0 drops U0). */
+int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const double* Us_dev, double dt, const double* F_dev,
+                    double* Uout_dev, void* stream);
+
+/* One explicit step, in place on U_dev. ABL_STEP_EULER is PETSc's default explicit TS (forward Euler),
+ * which the reference's shock-tube tests run; ABL_STEP_SSPRK3 the three-stage strong-stability-
+ * preserving Runge-Kutta scheme (Shu-Osher form). Every stage fills the ghosts and evaluates the RHS at
+ * `precision`; the species are normalised after the step and the ghosts refilled. Single domain (a
+ * partitioned run exchanges halos between the stages and drives abl_fv_rk_stage itself). The step size
+ * policy (CFL step of the state the previous step started from, exact final time) is the caller's; see
+ * abl_fv_cfl_dt. */
+#define ABL_STEP_EULER 0
+#define ABL_STEP_SSPRK3 1
+int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, int precision, void* stream);
+
 /* Halo exchange between ranks of a partitioned mesh (the pack and unpack of DMGlobalToLocal's PetscSF
  * broadcast of the state to ghost/overlap cells, src/solver/timeStepper.cpp:343-344). Row i of a
  * width-column FP64 array is copied to or from a contiguous message buffer on `stream`:

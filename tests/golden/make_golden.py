@@ -11,6 +11,7 @@ Sources read (ABLATE 0.13.03):
   tests/unitTests/eos/perfectGasTests.cpp:91-236
   tests/unitTests/eos/tChemTests.cpp:259+           (+ tests/unitTests/inputs/eos/gri30.yaml NASA-7 data)
   tests/unitTests/eos/transport/sutherlandTests.cpp:143-145
+  tests/unitTests/finiteVolume/compressibleShockTubeTests.cpp:210+
 """
 from __future__ import annotations
 
@@ -227,6 +228,25 @@ def tchem(ref: Path) -> dict:
     return {"source": "tests/unitTests/eos/tChemTests.cpp", "mechanism": "gri30", "cases": cases}
 
 
+def shock_tube(ref: Path) -> dict:
+    """1D shock tubes: initial states, AUSM, nx cells, CFL, final time, and the expected primitives."""
+    src = (ref / "tests/unitTests/finiteVolume/compressibleShockTubeTests.cpp").read_text()
+    cases = []
+    for blk in _blocks(src, "CompressibleShockTubeParameters"):
+        name = re.search(r'MpiTestParameter\("([^"]+)"', blk).group(1)
+        ic_txt = _field(blk, "initialConditions")
+        ic = {k: _num(v) for k, v in re.findall(r"\.(\w+)\s*=\s*([^,}]+)", ic_txt)}
+        flux = re.search(r"fluxCalculator::(\w+)", _field(blk, "fluxCalculator")).group(1)
+        ev_txt = _field(blk, "expectedValues")
+        expected = {m.group(1): _list("{" + m.group(2) + "}") for m in re.finditer(r'\{"(\w+)",\s*\{([^}]*)\}\}', ev_txt)}
+        cases.append({"name": name, "initial": ic, "flux": flux, "nx": int(_num(_field(blk, "nx"))), "maxTime": _num(_field(blk, "maxTime")),
+                      "cfl": _num(_field(blk, "cfl")), "expected": expected})
+    return {"source": "tests/unitTests/finiteVolume/compressibleShockTubeTests.cpp",
+            "harness": "1D box [0, length], ghost cells holding the initial left/right state by face position, TS with "
+                       "ts_adapt_type physics, ts_adapt_safety 1, ts_exact_final_time matchstep, ASSERT_NEAR 1e-6",
+            "cases": cases}
+
+
 def main(argv):
     ref = Path(argv[1] if len(argv) > 1 else "/root/reference")
     out = {
@@ -236,6 +256,7 @@ def main(argv):
         "sutherland.json": sutherland(ref),
         "tchem_gri30.json": tchem(ref),
         "gri30_nasa7.json": gri30_thermo(ref),
+        "shock_tube.json": shock_tube(ref),
     }
     for name, data in out.items():
         text = json.dumps(data, indent=1, allow_nan=True)
