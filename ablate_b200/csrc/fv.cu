@@ -412,6 +412,28 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
         {
+            // cone-major geometry: per cone entry the LSQ state weight (0 across boundary faces and for
+            // cells without a state gradient), the aux weight and the neighbour offset x_n - x_c
+            const size_t ncone = h.cone_face.size();
+            std::vector<double> cw(3 * ncone, 0.0), caw(3 * ncone, 0.0), cv(3 * ncone, 0.0);
+            int maxc = 0;
+            for (int c = 0; c < h.n_cells; c++) {
+                maxc = std::max(maxc, h.cone_ptr[c + 1] - h.cone_ptr[c]);
+                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                    const int f = h.cone_face[i], sc = h.cone_side[i];
+                    for (int d = 0; d < 3; d++) {
+                        if (lsq && !h.face_boundary[f]) cw[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * sc + d];
+                        if (dif) caw[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * sc + d];
+                        cv[3 * (size_t)i + d] = h.fdx[6 * (size_t)f + 3 * sc + d] - h.fdx[6 * (size_t)f + 3 * (1 - sc) + d];
+                    }
+                }
+            }
+            fv->cw.upload(cw.data(), cw.size());
+            fv->caw.upload(caw.data(), caw.size());
+            fv->cv.upload(cv.data(), cv.size());
+            fv->max_cone = maxc;
+        }
+        {
             // per cell: sum of its LSQ weights over non-boundary faces, and of its aux weights over all
             std::vector<double> ws((size_t)h.n_cells * 6, 0.0);
             for (int c = 0; c < h.n_cells; c++)
@@ -505,6 +527,10 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.n_nonowned = (int)fv->nonowned.n;
         M.nonowned = fv->nonowned.p;
         M.wsum = fv->wsum.p;
+        M.cw = fv->cw.p;
+        M.caw = fv->caw.p;
+        M.cv = fv->cv.p;
+        M.max_cone = fv->max_cone;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();
     });

@@ -101,7 +101,8 @@ struct abl_fv {
     // adjoint work buffers, allocated on the first VJP
     abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb, adj_graw, adj_phi;
     abl::DevBuf<int> adj_fstar, adj_ist;
-    abl::DevBuf<double> wsum;
+    abl::DevBuf<double> wsum, cw, caw, cv;
+    int max_cone = 0;
     // boundary ghosts and time stepping
     int n_ghost = 0;
     abl::DevBuf<int> ghost_cell, ghost_nbr, ghost_bc;

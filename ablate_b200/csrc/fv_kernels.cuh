@@ -56,6 +56,12 @@ struct DevMesh {
     int n_nonowned;
     const int* nonowned;  // cells that are not owned (boundary ghosts, halos)
     const double* wsum;   // [nc][2][3] per cell: sum of its LSQ state weights (non-boundary faces), of its aux weights
+    // per cone entry (cell-major, contiguous per cell): LSQ state weight (0 across a boundary face),
+    // aux (face-interpolant) weight, and the neighbour offset x_n - x_c
+    const double* cw;
+    const double* caw;
+    const double* cv;
+    int max_cone;
 };
 
 template <int DIM, int NS>
@@ -73,12 +79,13 @@ struct GradRows {
     static constexpr int AS = ((Dims<DIM, NS>::NA * DIM + V - 1) / V) * V;
 };
 
-// minimum resident CTAs per SM for __launch_bounds__ (register budget per thread = 65536 / (128 * n)):
-// FP32 reconstruction fits 6 gradient CTAs, FP64 4, the value+tangent pairs of the tangent kernels 1
+// minimum resident CTAs per SM for __launch_bounds__ (register budget per thread = 65536 / (128 * n)),
+// chosen by timing on the 128^3 case: gradient FP64 4 / FP32 6, tile FP64 4 (no spills at 128
+// registers) / FP32 5; the value+tangent pairs of the tangent kernels 1
 template <int NS, class G>
 struct MinBlocks {
     static constexpr int grad = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : (NS > 0 ? 3 : (sizeof(G) == 8 ? 4 : 6)));
-    static constexpr int tile = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : 3);
+    static constexpr int tile = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : (sizeof(G) == 8 ? 4 : 5));
 };
 
 constexpr int kConeSide = int(1u << 31);
@@ -214,10 +221,12 @@ __global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __
 // cellInterpolant.cpp:282-328, and the cancel rule at :459-481)
 // REC (the adjoint's forward pass) also records, per component, the applied factor (0 when the
 // gradient was cancelled) and the cone entry of the minimising face (-1: none, or cancelled).
+// sd, when not null, holds the cell's neighbour differences u_n - u_c per cone entry (written by the
+// gradient pass; thread-interleaved) so the neighbour states are not read again.
 template <int DIM, int NS, class G, int LIM, bool REC = false>
 __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U,
                                             const double* __restrict__ dU, const StateOf<G>* uc, G* g, int k0, int k1,
-                                            double* rphi = nullptr, int* rist = nullptr) {
+                                            double* rphi = nullptr, int* rist = nullptr, const G* sd = nullptr) {
     using D = Dims<DIM, NS>;
     using S = StateOf<G>;
     G phi[D::NC];
@@ -229,21 +238,19 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
     }
 #pragma unroll 2
     for (int i = beg; i < end; i++) {
-        const int2 ce = M.cone[i];
-        const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
-        // x_n - x_c = (x_f - x_c) - (x_f - x_n), each offset taken in its own cell's frame
+        // x_n - x_c, periodic images resolved (face offsets taken in each cell's own frame)
         G v[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; d++) v[d] = G(__ldg(M.fdx + 6 * (size_t)f + 3 * sc + d) - __ldg(M.fdx + 6 * (size_t)f + 3 * (1 - sc) + d));
+        for (int d = 0; d < DIM; d++) v[d] = G(__ldg(M.cv + 3 * (size_t)i + d));
         S un[D::NC];
-        load_state<DIM, NS, S>(U, dU, n, un);
+        if (!sd) load_state<DIM, NS, S>(U, dU, M.cone[i].y & kConeNbr, un);
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
             if (k < k0 || k >= k1) continue;
             G denom = 0;
 #pragma unroll
             for (int d = 0; d < DIM; d++) denom += g[k * DIM + d] * v[d];
-            const G diff = G(un[k] - uc[k]);
+            const G diff = sd ? sd[((i - beg) * D::NC + k) * blockDim.x + threadIdx.x] : G(un[k] - uc[k]);
             const G flim = G(0.5) * diff * rcp64(denom);
             if constexpr (REC) {
                 const G l = limiter_k<LIM, G>(P.limiter, flim);
@@ -286,8 +293,9 @@ template <int DIM, int NS, class G, int LIM, bool REC = false>
 __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMesh M, Phys P, const double* __restrict__ U,
                                                                     const double* __restrict__ dU, const double* __restrict__ aux,
                                                                     G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux,
-                                                                    G* __restrict__ graw = nullptr, double* __restrict__ rphi = nullptr,
+                                                                    int cache, G* __restrict__ graw = nullptr, double* __restrict__ rphi = nullptr,
                                                                     int* __restrict__ rist = nullptr) {
+    extern __shared__ __align__(16) unsigned char gsm[];
     using D = Dims<DIM, NS>;
     using GR = GradRows<DIM, NS, G>;
     using S = StateOf<G>;
@@ -306,17 +314,23 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
     for (int k = 0; k < D::NC * DIM; k++) g[k] = G(0);
 #pragma unroll
     for (int k = 0; k < D::NA * DIM; k++) ga[k] = G(0);
+    // neighbour differences kept for the limiter when the block has shared memory for them
+    G* sd = (cache && state && P.limiter != ABL_LIMITER_NONE && end - beg <= M.max_cone) ? reinterpret_cast<G*>(gsm) : nullptr;
     if (state || auxg) {
 #pragma unroll 2
         for (int i = beg; i < end; i++) {
             const int2 ce = M.cone[i];
-            const int f = ce.x, n = ce.y & kConeNbr, sc = (ce.y & kConeSide) ? 1 : 0;
+            const int n = ce.y & kConeNbr;
             S un[D::NC];
             if (state || !nasa || std::is_same<S, Dual>::value) load_state<DIM, NS, S>(U, dU, n, un);
+            if (sd) {
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) sd[((i - beg) * D::NC + k) * blockDim.x + threadIdx.x] = G(un[k] - uc[k]);
+            }
             if (state && !(ce.y & kConeBoundary)) {
                 G wd[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.cgrad + 6 * (size_t)f + 3 * sc + d));
+                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.cw + 3 * (size_t)i + d));
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) {
                     const G delta = G(un[k] - uc[k]);
@@ -329,7 +343,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 cell_aux<DIM, NS>(P, un, aux, n, an);
                 G wd[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.fgrad + 6 * (size_t)f + 3 * sc + d));
+                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.caw + 3 * (size_t)i + d));
 #pragma unroll
                 for (int k = 0; k < D::NA; k++) {
                     const G delta = G(an[k] - ac[k]);
@@ -353,8 +367,8 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 for (int k = 0; k < D::NC * DIM; k++) o[k] = g[k];
             }
             if (state && P.limiter != ABL_LIMITER_NONE) {
-                limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, 0, D::NE, ph, is);
-                if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, ph, is);
+                limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, 0, D::NE, ph, is, sd);
+                if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, ph, is, sd);
             }
             if (do_state) {
 #pragma unroll
@@ -364,8 +378,8 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 }
             }
         } else if (state && P.limiter != ABL_LIMITER_NONE) {
-            limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, 0, D::NE);
-            if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC);
+            limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, 0, D::NE, nullptr, nullptr, sd);
+            if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, nullptr, nullptr, sd);
         }
     }
     if (do_state) {

@@ -16,10 +16,18 @@ void launch_tile(abl_fv* fv, const double* U, const double* dU, const G* grad, c
     check_launch();
 }
 
+// shared memory for the neighbour differences the limiter reuses (none when it would not fit)
+template <int DIM, int NS, class G>
+size_t gradient_smem(const abl_fv* fv) {
+    const size_t b = (size_t)128 * fv->mesh.max_cone * Dims<DIM, NS>::NC * sizeof(G);
+    return b <= 48 * 1024 ? b : 0;
+}
+
 template <int DIM, int NS, class G, int LIM>
 void launch_gradient(abl_fv* fv, const double* U, const double* dU, G* grad, G* agrad, cudaStream_t s) {
-    k_gradient<DIM, NS, G, LIM><<<blocks_for(fv->mesh.n_cells, 128), 128, 0, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad,
-                                                                                  fv->need_state_grad, fv->need_aux_grad);
+    const size_t smem = gradient_smem<DIM, NS, G>(fv);
+    k_gradient<DIM, NS, G, LIM><<<blocks_for(fv->mesh.n_cells, 128), 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad,
+                                                                                  fv->need_state_grad, fv->need_aux_grad, smem > 0);
     check_launch();
 }
 
@@ -106,8 +114,9 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
     if (fv->need_state_grad || fv->need_aux_grad) {
         mark(fv, "k_gradient", s);
         auto kern = P.limiter == ABL_LIMITER_MINMOD ? k_gradient<DIM, NS, double, ABL_LIMITER_MINMOD, true> : k_gradient<DIM, NS, double, -1, true>;
-        kern<<<blocks_for(M.n_cells, 128), 128, 0, s>>>(M, P, U, nullptr, fv->aux.p, fv->grad64.p, fv->agrad64.p, fv->need_state_grad,
-                                                       fv->need_aux_grad, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p);
+        const size_t smem = gradient_smem<DIM, NS, double>(fv);
+        kern<<<blocks_for(M.n_cells, 128), 128, smem, s>>>(M, P, U, nullptr, fv->aux.p, fv->grad64.p, fv->agrad64.p, fv->need_state_grad,
+                                                          fv->need_aux_grad, smem > 0, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p);
         check_launch();
     }
     AdjOut<DIM, NS> out{fv->need_state_grad ? fv->adj_gb.p : nullptr, fv->adj_beta.p, fv->adj_fstar.p,
