@@ -236,7 +236,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
         phi[k] = big_value<G>();
         ist[k] = -1;
     }
-#pragma unroll 2
+#pragma unroll 1
     for (int i = beg; i < end; i++) {
         // x_n - x_c, periodic images resolved (face offsets taken in each cell's own frame)
         G v[DIM];
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
     // neighbour differences kept for the limiter when the block has shared memory for them
     G* sd = (cache && state && P.limiter != ABL_LIMITER_NONE && end - beg <= M.max_cone) ? reinterpret_cast<G*>(gsm) : nullptr;
     if (state || auxg) {
-#pragma unroll 2
+#pragma unroll 1
         for (int i = beg; i < end; i++) {
             const int2 ce = M.cone[i];
             const int n = ce.y & kConeNbr;

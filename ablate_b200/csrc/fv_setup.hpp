@@ -6,8 +6,10 @@
 //     (fg->grad[side]: pseudo-inverse of each cell's neighbour offsets over its non-boundary faces)
 //   LeastSquaresAverage::ComputeNeighborCellStencil  src/finiteVolume/stencils/leastSquaresAverage.cpp:71-148
 //     (per-cell gradient operator over every two-sided face, used for face gradients of aux fields)
-// The pseudo-inverse is computed by Householder QR of the offset matrix (full column rank) or by the
-// minimum-norm formula B^T (B B^T)^-1 (fewer offsets than dimensions: a boundary ghost cell).
+// The pseudo-inverse is computed by Householder QR of the offset matrix (full column rank), by the
+// minimum-norm formula B^T (B B^T)^-1 (fewer offsets than dimensions: a boundary ghost cell), or, for
+// offsets spanning fewer directions (cells next to the boundary of a tetrahedral mesh), from the
+// eigen-decomposition of B^T B with the null directions dropped.
 #pragma once
 #include "fv_consts.hpp"
 #include <algorithm>
@@ -36,9 +38,65 @@ struct HostMesh {
     std::vector<double> fdx;             // [nf][2][3] face centroid minus side-s cell centroid, in that cell's frame
 };
 
+// Pseudo-inverse through the eigen-decomposition of B^T B (cyclic Jacobi rotations), eigenvalues
+// below 1e-14 of the largest treated as zero: the minimum-norm least-squares operator of a
+// rank-deficient stencil (the SVD least squares PetscFVComputeGradient uses, restated).
+inline void lsq_pinv_eig(int n, int dim, const double* B, double* W) {
+    double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int i = 0; i < n; i++)
+        for (int a = 0; a < dim; a++)
+            for (int b = 0; b < dim; b++) A[a][b] += B[i * dim + a] * B[i * dim + b];
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0;
+        for (int a = 0; a < dim; a++)
+            for (int b = a + 1; b < dim; b++) off += A[a][b] * A[a][b];
+        if (off < 1e-300) break;
+        for (int p = 0; p < dim; p++)
+            for (int q = p + 1; q < dim; q++) {
+                if (A[p][q] == 0.0) continue;
+                const double th = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < dim; k++) {  // A <- A J
+                    const double x = A[k][p], y = A[k][q];
+                    A[k][p] = c * x - sn * y;
+                    A[k][q] = sn * x + c * y;
+                }
+                for (int k = 0; k < dim; k++) {  // A <- J^T A
+                    const double x = A[p][k], y = A[q][k];
+                    A[p][k] = c * x - sn * y;
+                    A[q][k] = sn * x + c * y;
+                }
+                for (int k = 0; k < dim; k++) {
+                    const double x = V[k][p], y = V[k][q];
+                    V[k][p] = c * x - sn * y;
+                    V[k][q] = sn * x + c * y;
+                }
+            }
+    }
+    double lmax = 0;
+    for (int a = 0; a < dim; a++) lmax = std::max(lmax, A[a][a]);
+    double Mi[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // (B^T B)^+
+    for (int a = 0; a < dim; a++) {
+        if (!(A[a][a] > 1e-14 * lmax)) continue;
+        for (int r = 0; r < dim; r++)
+            for (int s2 = 0; s2 < dim; s2++) Mi[r][s2] += V[r][a] * V[s2][a] / A[a][a];
+    }
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < dim; d++) {
+            double acc = 0;
+            for (int e = 0; e < dim; e++) acc += Mi[d][e] * B[i * dim + e];
+            W[i * dim + d] = acc;
+        }
+}
+
 // Pseudo-inverse of B (n x dim, row-major) returned as W (n x dim) with W[i][:] = pinv(B)[:, i].
+// Full column rank: Householder QR; fewer offsets than dimensions: B^T (B B^T)^-1; a stencil whose
+// offsets span fewer than min(n, dim) directions: lsq_pinv_eig.
 inline void lsq_pinv(int n, int dim, const double* B, double* W) {
     if (n >= dim) {
+        // numerical rank from the diagonal of R below
+        bool deficient = false;
         // Householder QR: B = Q R, pinv(B) = R^-1 Q^T
         std::vector<double> A(B, B + (size_t)n * dim);  // row-major n x dim
         std::vector<double> vs((size_t)dim * n, 0.0);
@@ -47,7 +105,10 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
             double norm = 0;
             for (int i = j; i < n; i++) norm += A[i * dim + j] * A[i * dim + j];
             norm = std::sqrt(norm);
-            if (norm == 0.0) throw std::runtime_error("rank-deficient least-squares stencil");
+            if (norm == 0.0) {
+                deficient = true;
+                break;
+            }
             double alpha = A[j * dim + j] > 0 ? -norm : norm;
             double* v = &vs[(size_t)j * n];
             for (int i = 0; i < n; i++) v[i] = 0;
@@ -62,6 +123,16 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
                 s *= beta[j];
                 for (int i = j; i < n; i++) A[i * dim + k] -= s * v[i];
             }
+        }
+        double rmax = 0;
+        if (!deficient)
+            for (int j = 0; j < dim; j++) rmax = std::max(rmax, std::fabs(A[j * dim + j]));
+        if (!deficient)
+            for (int j = 0; j < dim; j++)
+                if (!(std::fabs(A[j * dim + j]) > 1e-7 * rmax)) deficient = true;
+        if (deficient) {
+            lsq_pinv_eig(n, dim, B, W);
+            return;
         }
         // columns of pinv: solve R x = (Q^T e_i)[0:dim] for each i
         std::vector<double> q(n);
@@ -93,6 +164,10 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
             Gi[0][0] = 1.0 / G[0][0];
         } else {
             double det = G[0][0] * G[1][1] - G[0][1] * G[1][0];
+            if (!(std::fabs(det) > 1e-14 * G[0][0] * G[1][1])) {  // parallel offsets
+                lsq_pinv_eig(n, dim, B, W);
+                return;
+            }
             Gi[0][0] = G[1][1] / det;
             Gi[1][1] = G[0][0] / det;
             Gi[0][1] = -G[0][1] / det;

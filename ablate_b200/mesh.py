@@ -174,3 +174,73 @@ def ghost_interior_map(mesh: Mesh) -> np.ndarray:
     for i, c in enumerate(g.tolist()):
         out[i] = out_map[c]
     return out
+
+
+def delaunay_mesh(n_cells: int, extent=(1.0, 0.2, 0.2), seed: int = 20261205, jitter: float = 0.3) -> Mesh:
+    """Tetrahedral mesh of the box [0, extent] from the Delaunay triangulation of a seeded point cloud
+    (a lattice of spacing h jittered by up to jitter*h, with the box corners and the lattice points on
+    the box faces held on the faces, so the tetrahedra fill the box), with one FV ghost cell behind
+    every boundary face (centroid reflected through the face centroid, the interior volume).
+    n_cells sets the lattice spacing; the tetrahedron count comes out near it. Cells are ordered along
+    a Morton curve of their centroids."""
+    from scipy.spatial import Delaunay
+
+    ext = np.asarray(extent, float)
+    # about 3.9 tetrahedra per lattice cell for a jittered lattice
+    h = (float(np.prod(ext)) * 3.9 / n_cells) ** (1.0 / 3.0)
+    shape = np.maximum(1, np.round(ext / h).astype(int))
+    axes = [np.linspace(0.0, ext[a], shape[a] + 1) for a in range(3)]
+    P = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    hs = ext / shape
+    J = rng.uniform(-jitter, jitter, P.shape) * hs
+    on_face = (np.isclose(P, 0.0) | np.isclose(P, ext))  # keep boundary points on their faces
+    J[on_face] = 0.0
+    P = P + J
+    tri = Delaunay(P)
+    tets = tri.simplices.astype(np.int64)
+    V = P[tets]  # (nt, 4, 3)
+    vol6 = np.einsum("ij,ij->i", V[:, 1] - V[:, 0], np.cross(V[:, 2] - V[:, 0], V[:, 3] - V[:, 0]))
+    keep = np.abs(vol6) > 1e-12 * float(np.prod(hs))  # drop flat boundary slivers
+    tets, V, vol6 = tets[keep], V[keep], vol6[keep]
+    cc = V.mean(1)
+    # Morton order of the cells
+    q = ((cc / ext) * ((1 << 20) - 1)).astype(np.int64).T
+    perm = np.argsort(_morton_keys(q, 3), kind="stable")
+    tets, V, vol6, cc = tets[perm], V[perm], vol6[perm], cc[perm]
+    nt = tets.shape[0]
+    # faces: the 4 vertex triples of every tet, matched by their sorted vertex ids
+    tri_idx = np.array([[1, 2, 3], [0, 2, 3], [0, 1, 3], [0, 1, 2]])
+    F = np.sort(tets[:, tri_idx].reshape(-1, 3), axis=1)
+    owner = np.repeat(np.arange(nt), 4)
+    key = (F[:, 0] * P.shape[0] + F[:, 1]) * P.shape[0] + F[:, 2]
+    order = np.argsort(key, kind="stable")
+    ks, os_ = key[order], owner[order]
+    same = np.nonzero(ks[1:] == ks[:-1])[0]
+    inner = np.zeros(ks.size, bool)
+    inner[same] = inner[same + 1] = True
+    pairs = np.stack([os_[same], os_[same + 1]], 1)
+    bnd_pos = order[~inner]
+    bnd_cells = owner[bnd_pos]
+    tri_int = F[order[same]]
+    tri_bnd = F[bnd_pos]
+    # interior faces (left = smaller cell id), then boundary faces with their ghosts
+    L_, R_ = pairs.min(1), pairs.max(1)
+    nb = bnd_cells.size
+    ghosts = nt + np.arange(nb)
+    face_cells = np.concatenate([np.stack([L_, R_], 1), np.stack([bnd_cells, ghosts], 1)])
+    tris = np.concatenate([tri_int, tri_bnd])
+    Pt = P[tris]
+    fcen = Pt.mean(1)
+    nrm = 0.5 * np.cross(Pt[:, 1] - Pt[:, 0], Pt[:, 2] - Pt[:, 0])
+    gcen = 2.0 * fcen[L_.size:] - cc[bnd_cells]
+    cell_centroid = np.concatenate([cc, gcen])
+    # orient every normal from left to right
+    d = cell_centroid[face_cells[:, 1]] - cell_centroid[face_cells[:, 0]]
+    nrm[np.einsum("ij,ij->i", nrm, d) < 0] *= -1.0
+    fo = np.lexsort((face_cells[:, 1], face_cells[:, 0]))
+    cell_volume = np.concatenate([np.abs(vol6) / 6.0, np.abs(vol6[bnd_cells]) / 6.0])
+    kind = np.zeros(nt + nb, np.uint8)
+    kind[nt:] = L.CELL_BOUNDARY
+    return Mesh(dim=3, face_cells=face_cells[fo].astype(np.int32), face_normal=nrm[fo], face_centroid=fcen[fo],
+                cell_centroid=cell_centroid, cell_volume=cell_volume, cell_kind=kind, face_shift=None, n_interior=nt, shape=())

@@ -24,7 +24,7 @@ import numpy as np
 
 from . import _lib as L
 from . import fv
-from .mesh import Mesh, box_mesh, ghost_interior_map
+from .mesh import Mesh, box_mesh, delaunay_mesh, ghost_interior_map
 
 
 @dataclass
@@ -202,6 +202,37 @@ def shear3d(n: int = 256, ns: int = 5, seed: int = 20261205, diffusion: bool = F
                  fv.SpeciesTransport(eos, flux, fv.ConstantLewis(1.8e-5, 0.72, 1.0))]
     return Workload("shear3d", mesh, eos, procs, "leastsquares", "minmod", U,
                     f"3D Euler + {ns} species {n}^3 hex, NASA-7 mixture, tanh shear layer (ratio 3), AUSM+up + LSQ + minmod")
+
+
+def channel_tets(n: int = 2_000_000, ns: int = 9, seed: int = 20261205) -> Workload:
+    """Reacting-flow transport without chemistry on a seeded Delaunay tetrahedral mesh of the
+    1 x 0.2 x 0.2 channel (about n cells): ns species with seeded NASA-7 data (cp/R in 2.5-6 over
+    300-3000 K), mass fractions from layered profiles mixed with a seeded Dirichlet draw, T in
+    300-2500 K (a hot core with 2 % seeded noise), p = 1 atm, a seeded velocity field; AUSM+up, least
+    squares + van Leer, constant Lewis number 1 diffusion."""
+    from .mesh import delaunay_mesh
+    mesh = delaunay_mesh(n, seed=seed)
+    rng = np.random.default_rng(seed)
+    eos = synthetic_mixture(ns, seed)
+    nc = mesh.n_cells
+    x = mesh.cell_centroid
+    # a hot core and layered composition with seeded cell-to-cell noise: T spans 300-2500 K
+    r2 = ((x[:, 1] - 0.1) ** 2 + (x[:, 2] - 0.1) ** 2) / 0.01
+    T = 300.0 + 2200.0 * np.exp(-2.0 * r2) * (0.6 + 0.4 * np.sin(2 * np.pi * x[:, 0])) ** 2
+    T *= 1.0 + 0.02 * rng.standard_normal(nc)
+    T = np.clip(T, 300.0, 2500.0)
+    Ylayer = np.stack([1.0 + np.cos(2 * np.pi * (k + 1) * x[:, 0] + k) for k in range(ns)], 1) + 0.2
+    Y = 0.8 * Ylayer / Ylayer.sum(1, keepdims=True) + 0.2 * rng.dirichlet(np.ones(ns) * 2.0, nc)
+    W = 1.0 / (Y / eos.mw).sum(1)
+    rho = 101325.0 * W / (8314.46261815324 * T)
+    vel = np.stack([30.0 * np.sin(2 * np.pi * x[:, 1] / 0.2), 10.0 * np.cos(2 * np.pi * x[:, 0]), 5.0 * np.ones(nc)], 1)
+    vel += 2.0 * rng.standard_normal((nc, 3))
+    U = mixture_state(eos, rho, vel, T, Y)
+    flux = fv.AusmpUp(0.3)
+    tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
+    procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
+    return Workload("channel_tets", mesh, eos, procs, "leastsquares", "vanleer", U,
+                    f"3D {mesh.n_interior} seeded Delaunay tets in a 1x0.2x0.2 channel, {ns} NASA-7 species, AUSM+up + LSQ + van Leer, Le = 1")
 
 
 def initial_aux(w: Workload) -> np.ndarray:

@@ -81,6 +81,15 @@ def case(name: str) -> Workload:
         tr = fv.Constant(k=0.03, mu=2e-5, diff=1e-4)
         procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
         return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
+    if name.startswith("tets3d_"):
+        # seeded Delaunay tets of the 1 x 0.2 x 0.2 channel: variable cone sizes, ghosts on every side
+        if name == "tets3d_ns9":
+            return workloads.channel_tets(1500, 9, seed=zlib.crc32(name.encode()))
+        mesh = workloads.delaunay_mesh(1200, seed=zlib.crc32(name.encode()))
+        eos = fv.PerfectGas({"gamma": 1.4, "Rgas": 287.0})
+        U = _perturbed_state(mesh, rng, 3)
+        procs = [fv.NavierStokesTransport({}, eos, fv.Ausm(), fv.Constant(k=0.03, mu=2e-5))]
+        return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
     raise KeyError(name)
 
 
@@ -100,6 +109,8 @@ CASES = [
     "species3d_ns5",
     "species3d_ns9",
     "pgspecies3d_ns2",
+    "tets3d_ns9",
+    "tets3d_pg_minmod",
 ]
 
 

@@ -40,7 +40,8 @@ def test_row_gather_and_scatter_kernels():
         np.testing.assert_array_equal(dst.cpu().numpy(), ref)
 
 
-@pytest.mark.parametrize("name", ["tgv3d_ausmpup_lsq_minmod_visc", "sod2d_ausm_upwind", "species3d_ns5", "box2d_ausmpup_vanleer_suth"])
+@pytest.mark.parametrize("name", ["tgv3d_ausmpup_lsq_minmod_visc", "sod2d_ausm_upwind", "species3d_ns5", "box2d_ausmpup_vanleer_suth",
+                                  "tets3d_ns9"])
 @pytest.mark.parametrize("precision", [L.PRECISION_FP64, L.PRECISION_MIXED])
 def test_partitioned_device_rhs_equals_single_domain(name, precision):
     torch = pytest.importorskip("torch")

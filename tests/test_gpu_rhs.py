@@ -44,7 +44,7 @@ def test_rhs_fp64_matches_oracle(name):
         assert e <= FP64_TOL, f"{name} {block}: {e:.3e}"
 
 
-@pytest.mark.parametrize("name", ["tgv3d_mixed_check", "species3d_ns5", "box2d_ausmpup_vanleer_suth"])
+@pytest.mark.parametrize("name", ["tgv3d_mixed_check", "species3d_ns5", "box2d_ausmpup_vanleer_suth", "tets3d_ns9", "tets3d_pg_minmod"])
 def test_rhs_mixed_close_to_fp64(name):
     w = R.case(name)
     F64, _ = _run(w, L.PRECISION_FP64)

@@ -20,7 +20,8 @@ from ablate_b200.workloads import initial_aux
 from oracle import oracle as orc
 from tests import rhs_cases as R
 
-CASES = ["tgv3d_ausmpup_lsq_minmod_visc", "sod2d_ausm_upwind", "box2d_ausmpup_vanleer_suth", "species3d_ns5", "pgspecies3d_ns2"]
+CASES = ["tgv3d_ausmpup_lsq_minmod_visc", "sod2d_ausm_upwind", "box2d_ausmpup_vanleer_suth", "species3d_ns5", "pgspecies3d_ns2",
+         "tets3d_pg_minmod"]
 
 
 def _exchange_numpy(domains, plans, U_local):
