@@ -415,15 +415,21 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             // cone-major geometry: per cone entry the LSQ state weight (0 across boundary faces and for
             // cells without a state gradient), the aux weight and the neighbour offset x_n - x_c
             const size_t ncone = h.cone_face.size();
-            std::vector<double> cw(3 * ncone, 0.0), caw(3 * ncone, 0.0), cv(3 * ncone, 0.0);
+            std::vector<double> cw(3 * ncone, 0.0), caw(3 * ncone, 0.0), cv(3 * ncone, 0.0), cwr(3 * ncone, 0.0), cawr(3 * ncone, 0.0);
             int maxc = 0;
             for (int c = 0; c < h.n_cells; c++) {
                 maxc = std::max(maxc, h.cone_ptr[c + 1] - h.cone_ptr[c]);
                 for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
                     const int f = h.cone_face[i], sc = h.cone_side[i];
                     for (int d = 0; d < 3; d++) {
-                        if (lsq && !h.face_boundary[f]) cw[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * sc + d];
-                        if (dif) caw[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * sc + d];
+                        if (lsq && !h.face_boundary[f]) {
+                            cw[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * sc + d];
+                            cwr[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * (1 - sc) + d];
+                        }
+                        if (dif) {
+                            caw[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * sc + d];
+                            cawr[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * (1 - sc) + d];
+                        }
                         cv[3 * (size_t)i + d] = h.fdx[6 * (size_t)f + 3 * sc + d] - h.fdx[6 * (size_t)f + 3 * (1 - sc) + d];
                     }
                 }
@@ -431,6 +437,8 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             fv->cw.upload(cw.data(), cw.size());
             fv->caw.upload(caw.data(), caw.size());
             fv->cv.upload(cv.data(), cv.size());
+            fv->cwr.upload(cwr.data(), cwr.size());
+            fv->cawr.upload(cawr.data(), cawr.size());
             fv->max_cone = maxc;
         }
         {
@@ -455,11 +463,11 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         }
         if (lsq) {
             fv->grad64.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 2));
-            fv->grad32.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 4));
+            if (fv->ns == 0) fv->grad32.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 4));
         }
         if (dif) {
             fv->agrad64.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 2));
-            fv->agrad32.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 4));
+            if (fv->ns == 0) fv->agrad32.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 4));
         }
         fv->status.alloc(1);
         fv->status.zero();
@@ -530,6 +538,8 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.cw = fv->cw.p;
         M.caw = fv->caw.p;
         M.cv = fv->cv.p;
+        M.cwr = fv->cwr.p;
+        M.cawr = fv->cawr.p;
         M.max_cone = fv->max_cone;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();

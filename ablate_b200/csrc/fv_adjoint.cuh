@@ -932,12 +932,12 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
 #pragma unroll 1
     for (int i = M.cone_ptr[m]; i < M.cone_ptr[m + 1]; i++) {
         const int2 ce = M.cone[i];
-        const int f = ce.x, n = ce.y & kConeNbr, so = (ce.y & kConeSide) ? 0 : 1;  // so: the neighbour's side of f
+        const int f = ce.x, n = ce.y & kConeNbr;
         if (do_state) {
             if (!(ce.y & kConeBoundary)) {
                 double w[DIM], gn[D::NC * DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cgrad + 6 * (size_t)f + 3 * so + d);
+                for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cwr + 3 * (size_t)i + d);
                 load_row<D::NC * DIM, double>(in.gb + (size_t)n * GR::GS, gn);
 #pragma unroll
                 for (int k = 0; k < D::NC; k++)
@@ -951,7 +951,7 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
         if (do_aux) {
             double w[DIM], gn[D::NA * DIM];
 #pragma unroll
-            for (int d = 0; d < DIM; d++) w[d] = __ldg(M.fgrad + 6 * (size_t)f + 3 * so + d);
+            for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cawr + 3 * (size_t)i + d);
             load_row<D::NA * DIM, double>(in.gab + (size_t)n * GR::AS, gn);
 #pragma unroll
             for (int k = 0; k < D::NA; k++)

@@ -61,6 +61,10 @@ struct DevMesh {
     const double* cw;
     const double* caw;
     const double* cv;
+    // the same weights seen from the neighbour: per cone entry of c across face f, the neighbour's
+    // LSQ state weight and aux weight for f (the transposed operators of the adjoint gather)
+    const double* cwr;
+    const double* cawr;
     int max_cone;
 };
 

@@ -186,8 +186,8 @@ def delaunay_mesh(n_cells: int, extent=(1.0, 0.2, 0.2), seed: int = 20261205, ji
     from scipy.spatial import Delaunay
 
     ext = np.asarray(extent, float)
-    # about 3.9 tetrahedra per lattice cell for a jittered lattice
-    h = (float(np.prod(ext)) * 3.9 / n_cells) ** (1.0 / 3.0)
+    # about 6.6 tetrahedra per lattice point for a jittered lattice
+    h = (float(np.prod(ext)) * 6.6 / n_cells) ** (1.0 / 3.0)
     shape = np.maximum(1, np.round(ext / h).astype(int))
     axes = [np.linspace(0.0, ext[a], shape[a] + 1) for a in range(3)]
     P = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
@@ -197,7 +197,9 @@ def delaunay_mesh(n_cells: int, extent=(1.0, 0.2, 0.2), seed: int = 20261205, ji
     on_face = (np.isclose(P, 0.0) | np.isclose(P, ext))  # keep boundary points on their faces
     J[on_face] = 0.0
     P = P + J
-    tri = Delaunay(P)
+    # joggled input (QJ): Qhull perturbs the lattice's cospherical points instead of resolving them,
+    # five times faster here; the tetrahedra refer to the unperturbed points
+    tri = Delaunay(P, qhull_options="Qbb Qc Q12 QJ")
     tets = tri.simplices.astype(np.int64)
     V = P[tets]  # (nt, 4, 3)
     vol6 = np.einsum("ij,ij->i", V[:, 1] - V[:, 0], np.cross(V[:, 2] - V[:, 0], V[:, 3] - V[:, 0]))

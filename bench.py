@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "sod2d", "shear3d"])
+    ap.add_argument("--workload", default="tgv3d", choices=["tgv3d", "sod2d", "channel_tets", "shear3d"])
     ap.add_argument("--n", type=int, default=0, help="mesh cells per direction (default: the configuration's size)")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -57,6 +57,8 @@ def make_workload(name, n):
         return workloads.tgv3d(n or 128)
     if name == "sod2d":
         return workloads.sod2d(n or 256)
+    if name == "channel_tets":
+        return workloads.channel_tets(n or 2_000_000, 9)
     return workloads.shear3d(n or 256, 5)
 
 
@@ -327,6 +329,33 @@ def main():
         vjp_ms, kernels["vjp"] = timed(lambda: solver.ComputeVJPDevice(0.0, U.data_ptr(), Fbar.data_ptr(), Ubar.data_ptr(), stream.cuda_stream),
                                        "VJP")
 
+    # the 2D Euler configuration also marches: 100 SSP-RK3 steps at CFL 0.5 with the CFL step of each
+    # state, ghosts filled before every stage (one RHS was timed above)
+    march = None
+    head_prec = L.PRECISION_FP64 if L.PRECISION_FP64 in results else precisions[0]
+    if w.name == "sod2d" and world == 1:
+        Um = U.clone()
+        for _ in range(2):
+            dt = solver.CflTimeStepDevice(Um.data_ptr(), 0.5, stream.cuda_stream)
+            solver.StepDevice(L.STEP_SSPRK3, 0.0, dt, Um.data_ptr(), head_prec, stream.cuda_stream)
+        Um.copy_(U)
+        torch.cuda.synchronize(dev)
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        t_sim = 0.0
+        for _ in range(100):
+            dt = solver.CflTimeStepDevice(Um.data_ptr(), 0.5, stream.cuda_stream)
+            solver.StepDevice(L.STEP_SSPRK3, t_sim, dt, Um.data_ptr(), head_prec, stream.cuda_stream)
+            t_sim += dt
+        m1.record(stream)
+        torch.cuda.synchronize(dev)
+        if solver.Status() != L.OK:
+            raise RuntimeError("device status after the march")
+        ms = m0.elapsed_time(m1)
+        march = {"steps": 100, "scheme": "ssprk3", "cfl": 0.5, "ms": ms, "ms_per_step": ms / 100,
+                 "mcell_per_s": 300 * int(w.mesh.n_interior) / (ms * 1e-3) / 1e6, "t_end": t_sim,
+                 "note": "per step: CFL step (device minimum, read back), 3 stages of ghost fill + RHS + stage update"}
+
     # accuracy of the mixed path against FP64 on this workload
     mixed_err = None
     if L.PRECISION_MIXED in results:
@@ -412,6 +441,7 @@ def main():
                 "h2d_bytes_per_step": (state_bytes if world > 1 else 2 * state_bytes), "d2h_bytes_per_step": state_bytes, "ms_per_step": e2e_ms,
                 "path": ("per rank: pinned host U copied in, halo exchange + RHS, F copied out, every step" if world > 1 else
                          "abl_fv_rhs_host: pinned host U and F copied in, RHS, F copied out, every step")},
+        "march": march,
         "gpu_launches": launches,
         "clocks": clocks,
     }
