@@ -32,15 +32,16 @@ ABL_HD R pmax(R a, R b) { return a < b ? b : a; }
 template <class R>
 ABL_HD R sqr(R a) { return a * a; }
 
-// FP64 reciprocal from an FP32 seed and two Newton steps (relative error below one ulp of the result
-// for |x| in the FP32 normal range); zero, subnormal-in-FP32, infinite, NaN and out-of-range inputs
-// take the IEEE division so their special values are exactly those of 1/x.
+// FP64 reciprocal: the hardware approximation of PTX rcp.approx.ftz.f64 (relative error about 2^-23)
+// refined by two Newton-Raphson steps r <- r (2 - x r), each squaring the relative error, to below one
+// ulp. Zero, infinite, NaN and extreme inputs (|x| outside 1e-300..1e300, where the approximation
+// flushes subnormals) take the IEEE division, so their special values are exactly those of 1/x.
 ABL_HD double rcp64(double x) {
 #ifdef __CUDA_ARCH__
-    const float xf = __double2float_rn(x);
-    const float ax = fabsf(xf);
-    if (!(ax > 1.2e-38f && ax < 3.0e38f)) return 1.0 / x;
-    double r = (double)__frcp_rn(xf);
+    const double ax = fabs(x);
+    if (!(ax > 1e-300 && ax < 1e300)) return 1.0 / x;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
     r = r * fma(-x, r, 2.0);
     r = r * fma(-x, r, 2.0);
     return r;
