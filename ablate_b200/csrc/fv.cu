@@ -439,6 +439,16 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             fv->cv.upload(cv.data(), cv.size());
             fv->cwr.upload(cwr.data(), cwr.size());
             fv->cawr.upload(cawr.data(), cawr.size());
+            if (fv->ns == 0) {  // the mixed path's copies (with species it runs the FP64 kernels)
+                std::vector<float> f32(cw.begin(), cw.end());
+                fv->cw32.upload(f32.data(), f32.size());
+                f32.assign(caw.begin(), caw.end());
+                fv->caw32.upload(f32.data(), f32.size());
+                f32.assign(cv.begin(), cv.end());
+                fv->cv32.upload(f32.data(), f32.size());
+                f32.assign(tl.tf_fdx.begin(), tl.tf_fdx.end());
+                fv->tf_fdx32.upload(f32.data(), f32.size());
+            }
             fv->max_cone = maxc;
         }
         {
@@ -540,6 +550,10 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.cv = fv->cv.p;
         M.cwr = fv->cwr.p;
         M.cawr = fv->cawr.p;
+        M.cw32 = fv->cw32.p;
+        M.caw32 = fv->caw32.p;
+        M.cv32 = fv->cv32.p;
+        M.tf_fdx32 = fv->tf_fdx32.p;
         M.max_cone = fv->max_cone;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();

@@ -66,7 +66,22 @@ struct DevMesh {
     const double* cwr;
     const double* cawr;
     int max_cone;
+    // FP32 copies of the weights and offsets the mixed path rounds to FP32 anyway (identical results,
+    // half the bytes): cw, caw, cv and the tile-face offsets
+    const float* cw32;
+    const float* caw32;
+    const float* cv32;
+    const float* tf_fdx32;
 };
+
+// a geometry value in the reconstruction type G: the FP32 copy for the mixed path
+template <class G>
+__device__ __forceinline__ G geo(const double* __restrict__ p64, const float* __restrict__ p32, size_t i) {
+    if constexpr (std::is_same<G, float>::value)
+        return __ldg(p32 + i);
+    else
+        return G(__ldg(p64 + i));
+}
 
 template <int DIM, int NS>
 struct Dims {
@@ -245,7 +260,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
         // x_n - x_c, periodic images resolved (face offsets taken in each cell's own frame)
         G v[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; d++) v[d] = G(__ldg(M.cv + 3 * (size_t)i + d));
+        for (int d = 0; d < DIM; d++) v[d] = geo<G>(M.cv, M.cv32, 3 * (size_t)i + d);
         S un[D::NC];
         if (!sd) load_state<DIM, NS, S>(U, dU, M.cone[i].y & kConeNbr, un);
 #pragma unroll
@@ -334,7 +349,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
             if (state && !(ce.y & kConeBoundary)) {
                 G wd[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.cw + 3 * (size_t)i + d));
+                for (int d = 0; d < DIM; d++) wd[d] = geo<G>(M.cw, M.cw32, 3 * (size_t)i + d);
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) {
                     const G delta = G(un[k] - uc[k]);
@@ -347,7 +362,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 cell_aux<DIM, NS>(P, un, aux, n, an);
                 G wd[DIM];
 #pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = G(__ldg(M.caw + 3 * (size_t)i + d));
+                for (int d = 0; d < DIM; d++) wd[d] = geo<G>(M.caw, M.caw32, 3 * (size_t)i + d);
 #pragma unroll
                 for (int k = 0; k < D::NA; k++) {
                     const G delta = G(an[k] - ac[k]);
@@ -697,8 +712,8 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
         for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_normal + 3 * (size_t)i + d);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            fdx[d] = __ldg(M.tf_fdx + 6 * (size_t)i + d);
-            fdx[3 + d] = __ldg(M.tf_fdx + 6 * (size_t)i + 3 + d);
+            fdx[d] = std::is_same<G, float>::value ? double(__ldg(M.tf_fdx32 + 6 * (size_t)i + d)) : __ldg(M.tf_fdx + 6 * (size_t)i + d);
+            fdx[3 + d] = std::is_same<G, float>::value ? double(__ldg(M.tf_fdx32 + 6 * (size_t)i + 3 + d)) : __ldg(M.tf_fdx + 6 * (size_t)i + 3 + d);
         }
         S flux[D::NC];
         face_flux<DIM, NS, G, FK>(M, P, lr.x, lr.y, normal, fdx, U, dU, aux, grad, agrad, flux, &ok, &rok);

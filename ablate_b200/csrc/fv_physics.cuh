@@ -49,7 +49,13 @@ ABL_HD double rcp64(double x) {
     return 1.0 / x;
 #endif
 }
-ABL_HD float rcp64(float x) { return 1.0f / x; }
+ABL_HD float rcp64(float x) {
+#ifdef __CUDA_ARCH__
+    return __frcp_rn(x);  // IEEE round-to-nearest reciprocal without the general division path
+#else
+    return 1.0f / x;
+#endif
+}
 ABL_HD double dsqrt(double x) { return sqrt(x); }
 ABL_HD float dsqrt(float x) { return sqrtf(x); }
 ABL_HD double dabs(double x) { return fabs(x); }
