@@ -135,13 +135,17 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def read_traffic(workload: str, precision: str):
-    """DRAM bytes per RHS from the committed ncu summary (profiles/rhs_<workload>_traffic.txt), if any."""
-    p = ROOT / "profiles" / f"rhs_{workload}_traffic.txt"
+def read_traffic(workload: str, precision: str, kernel: str, n_cells: int):
+    """DRAM bytes per launch of one kernel from the committed ncu summary (profiles/traffic_<workload>.txt,
+    a line "cells: <n>" and lines "<precision> <kernel>: <bytes>"), if it has that kernel at this size."""
+    p = ROOT / "profiles" / f"traffic_{workload}.txt"
     if not p.exists():
         return None
-    for line in p.read_text().splitlines():
-        if line.startswith(f"{precision}_dram_bytes_per_rhs:"):
+    lines = p.read_text().splitlines()
+    if f"cells: {n_cells}" not in lines:
+        return None
+    for line in lines:
+        if line.startswith(f"{precision} {kernel}:"):
             return float(line.split(":")[1])
     return None
 
@@ -424,7 +428,7 @@ def main():
                                    f"({drhs.halo.bytes_per_exchange} B per rank per step)") if world > 1 else "single GPU",
                    "l2": "flushed (256 MiB write) between timed steps, outside the timed events"},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_achieved, "peak": peak, "unit": "GB/s", "frac": dom_achieved / peak,
-                     "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed"),
+                     "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed", dom_name, n_cells) if world == 1 else None,
                      "algorithmic_bytes_per_launch": B, "kernel_ms": dom_ms,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
                      "whole_rhs": {"achieved": achieved, "frac": achieved / peak, "ms": head_ms},
