@@ -96,6 +96,10 @@ SIGNATURES = {
                                         C.c_void_p]),
     "abl_fv_set_boundary": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, _ip]),
     "abl_fv_fill_ghosts": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
+    "abl_fv_fill_ghosts_jvp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_fill_ghosts_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_set_pressure_functional": (C.c_int, [C.c_void_p, C.c_int32, _ip, C.c_void_p]),
+    "abl_fv_pressure_functional": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_void_p]),
     "abl_fv_cfl_dt": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.POINTER(C.c_double), C.c_void_p]),
     "abl_fv_normalize_species": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_rk_stage": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,

@@ -14,7 +14,6 @@
 #include "fv_handle.hpp"
 #include "fv_setup.hpp"
 #include "fv_step.cuh"
-#include "fv_step.cuh"
 
 namespace abl {
 thread_local std::string g_last_error;
@@ -504,6 +503,22 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                 for (int d = 0; d < 3; d++) gnorm.push_back(d < h.dim ? sgn * n[d] / a : 0.0);
             }
             fv->n_ghost = (int)gc.size();
+            {
+                // segments of ghosts sharing an interior neighbour, ghosts ascending inside each
+                std::vector<int> order(gc.size());
+                for (size_t j = 0; j < order.size(); j++) order[j] = (int)j;
+                std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return gn[a] < gn[b]; });
+                std::vector<int> sp{0}, sn;
+                for (size_t q = 0; q < order.size(); q++) {
+                    if (q > 0 && gn[order[q]] != gn[order[q - 1]]) sp.push_back((int)q);
+                    if (q == 0 || gn[order[q]] != gn[order[q - 1]]) sn.push_back(gn[order[q]]);
+                }
+                if (!order.empty()) sp.push_back((int)order.size());
+                fv->n_gseg = (int)sn.size();
+                fv->gseg_ptr.upload(sp.data(), sp.size());
+                fv->gseg_nbr.upload(sn.data(), sn.size());
+                fv->gseg_ghost.upload(order.data(), order.size());
+            }
             fv->ghost_cell.upload(gc.data(), gc.size());
             fv->ghost_nbr.upload(gn.data(), gn.size());
             fv->ghost_bc.upload(gb.data(), gb.size());
@@ -908,6 +923,7 @@ int abl_fv_set_boundary(abl_fv* fv, int32_t n_bc, const abl_bc* table, const int
             }
         fv->bc_table.upload(table, n_bc);
         fv->ghost_bc.upload(gb.data(), gb.size());
+        fv->n_bc = n_bc;
     });
 }
 
@@ -921,6 +937,29 @@ template <int DIM, int NS>
 void run_fill_ghosts(abl_fv* fv, double* U, cudaStream_t s) {
     if (fv->n_ghost == 0) return;
     k_fill_ghosts<DIM, NS><<<blocks_for(fv->n_ghost, 256), 256, 0, s>>>(ghost_desc(fv), U);
+    check_launch();
+}
+template <int DIM, int NS>
+void run_fill_ghosts_jvp(abl_fv* fv, double* dU, cudaStream_t s) {
+    if (fv->n_ghost == 0) return;
+    k_fill_ghosts<DIM, NS, 1><<<blocks_for(fv->n_ghost, 256), 256, 0, s>>>(ghost_desc(fv), dU);
+    check_launch();
+}
+template <int DIM, int NS>
+void run_fill_ghosts_vjp(abl_fv* fv, double* Ub, cudaStream_t s) {
+    if (fv->n_ghost == 0) return;
+    const size_t n = (size_t)fv->n_ghost * fv->nc;
+    if (fv->ghost_vbar.n != n) fv->ghost_vbar.alloc(n);
+    k_fill_ghosts_vjp<DIM, NS><<<blocks_for(fv->n_gseg, 256), 256, 0, s>>>(
+        ghost_desc(fv), GhostSegments{fv->n_gseg, fv->gseg_ptr.p, fv->gseg_nbr.p, fv->gseg_ghost.p}, Ub, fv->ghost_vbar.p);
+    check_launch();
+    k_bc_value_reduce<><<<fv->n_bc, 256, 0, s>>>(fv->n_ghost, fv->ghost_bc.p, fv->nc, fv->ghost_vbar.p, fv->bc_vbar.p);
+    check_launch();
+}
+template <int DIM, int NS>
+void run_pressure_functional(abl_fv* fv, const double* U, double* Ub, cudaStream_t s) {
+    k_pressure_functional<DIM, NS><<<blocks_for(fv->fn_n, 256), 256, 0, s>>>(fv->phys, fv->fn_n, fv->fn_cells.p, fv->fn_w.p, U, fv->fn_partial.p,
+                                                                               Ub, fv->status.p);
     check_launch();
 }
 template <int DIM, int NS>
@@ -950,6 +989,67 @@ int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream) {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_fill_ghosts: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
         ABL_DISPATCH(fv, run_fill_ghosts, U_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !dU_dev) throw std::invalid_argument("abl_fv_fill_ghosts_jvp: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        ABL_DISPATCH(fv, run_fill_ghosts_jvp, dU_dev, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int abl_fv_fill_ghosts_vjp(abl_fv* fv, double* Ubar_dev, double* value_bar_host, void* stream) {
+    return guarded([&] {
+        if (!fv || !Ubar_dev) throw std::invalid_argument("abl_fv_fill_ghosts_vjp: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t nv = (size_t)fv->n_bc * ABL_BC_MAX_COMPONENTS;
+        if (fv->bc_vbar.n != nv) fv->bc_vbar.alloc(nv);
+        ABL_CUDA(cudaMemsetAsync(fv->bc_vbar.p, 0, nv * sizeof(double), s));
+        ABL_DISPATCH(fv, run_fill_ghosts_vjp, Ubar_dev, s);
+        if (value_bar_host) {
+            std::vector<double> vb(nv);
+            ABL_CUDA(cudaMemcpyAsync(vb.data(), fv->bc_vbar.p, nv * sizeof(double), cudaMemcpyDeviceToHost, s));
+            ABL_CUDA(cudaStreamSynchronize(s));
+            for (size_t k = 0; k < nv; k++) value_bar_host[k] += vb[k];
+        }
+    });
+}
+
+int abl_fv_set_pressure_functional(abl_fv* fv, int32_t n, const int32_t* cells, const double* weights) {
+    return guarded([&] {
+        if (!fv || n < 0 || (n > 0 && (!cells || !weights))) throw std::invalid_argument("abl_fv_set_pressure_functional: bad argument");
+        std::vector<uint8_t> seen(fv->n_cells, 0);
+        for (int j = 0; j < n; j++) {
+            if (cells[j] < 0 || cells[j] >= fv->n_cells)
+                throw std::invalid_argument("abl_fv_set_pressure_functional: cell " + std::to_string(cells[j]) + " out of range");
+            if (seen[cells[j]]++) throw std::invalid_argument("abl_fv_set_pressure_functional: cell " + std::to_string(cells[j]) + " listed twice");
+        }
+        ABL_CUDA(cudaSetDevice(fv->device));
+        fv->fn_n = n;
+        if (n == 0) return;
+        fv->fn_cells.upload(cells, n);
+        fv->fn_w.upload(weights, n);
+        fv->fn_partial.alloc(blocks_for(n, 256));
+    });
+}
+
+int abl_fv_pressure_functional(abl_fv* fv, const double* U_dev, double* J_host, double* Ubar_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev || !J_host) throw std::invalid_argument("abl_fv_pressure_functional: NULL argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        *J_host = 0.0;
+        if (fv->fn_n == 0) return;
+        ABL_DISPATCH(fv, run_pressure_functional, U_dev, Ubar_dev, s);
+        std::vector<double> part(blocks_for(fv->fn_n, 256));
+        ABL_CUDA(cudaMemcpyAsync(part.data(), fv->fn_partial.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ABL_CUDA(cudaStreamSynchronize(s));
+        double J = 0.0;
+        for (double v : part) J += v;
+        *J_host = J;
     });
 }
 

@@ -111,6 +111,15 @@ struct abl_fv {
     abl::DevBuf<abl_bc> bc_table;
     abl::DevBuf<unsigned long long> dt_bits;
     abl::DevBuf<double> step_U1, step_F;
+    // ghosts grouped by interior neighbour (adjoint of the fill), per-ghost value adjoints
+    int n_gseg = 0;
+    abl::DevBuf<int> gseg_ptr, gseg_nbr, gseg_ghost;
+    abl::DevBuf<double> ghost_vbar, bc_vbar;
+    int n_bc = 1;
+    // wall-pressure functional: distinct cells, weights, per-block partial sums
+    int fn_n = 0;
+    abl::DevBuf<int> fn_cells;
+    abl::DevBuf<double> fn_w, fn_partial;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;

@@ -8,7 +8,11 @@
 //   k_normalize_species  mass-fraction clipping after a step (SpeciesTransport::NormalizeSpecies,
 //                        src/finiteVolume/processes/speciesTransport.cpp:343-403)
 //   k_rk_stage           one Shu-Osher stage of the three-stage SSP Runge-Kutta scheme on the owned rows
+//   k_fill_ghosts_vjp    transpose of the ghost fill (adjoint of a march through time steps)
+//   k_bc_value_reduce    adjoint of the condition table values, summed per condition
+//   k_pressure_functional  J = sum_c w_c p(U_c) over a set of cells and its gradient dJ/dU
 #pragma once
+#include "fv_adjoint.cuh"
 #include "fv_kernels.cuh"
 
 namespace abl {
@@ -24,7 +28,9 @@ struct GhostBC {
     const abl_bc* table;
 };
 
-template <int DIM, int NS>
+// LIN = 1 is the tangent of the fill: the ghost's derivative with respect to its interior neighbour
+// (a Dirichlet value is a constant, so a plain Dirichlet ghost gets 0 and an enforced one -du).
+template <int DIM, int NS, int LIN = 0>
 __global__ void __launch_bounds__(256) k_fill_ghosts(GhostBC G, double* __restrict__ U) {
     using D = Dims<DIM, NS>;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -37,7 +43,7 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(GhostBC G, double* __restri
     switch (bc.kind) {
         case ABL_BC_DIRICHLET:
 #pragma unroll
-            for (int k = 0; k < D::NC; k++) u[k] = bc.enforce_at_face ? 2.0 * bc.value[k] - u[k] : bc.value[k];
+            for (int k = 0; k < D::NC; k++) u[k] = bc.enforce_at_face ? (LIN ? 0.0 : 2.0 * bc.value[k]) - u[k] : (LIN ? 0.0 : bc.value[k]);
             break;
         case ABL_BC_SLIP_WALL: {
             // reflect the normal momentum: (rho u)_g = (rho u)_i - 2 ((rho u)_i . n) n
@@ -134,6 +140,134 @@ __global__ void __launch_bounds__(256) k_rk_stage(const uint8_t* __restrict__ ki
     if (kind[e / nc] != ABL_CELL_OWNED) return;
     const double s = Us[e] + dt * F[e];
     Uout[e] = a == 0.0 ? b * s : a * U0[e] + b * s;
+}
+
+// Ghosts grouped by their interior neighbour: segment s owns ghosts seg_ghost[seg_ptr[s] .. seg_ptr[s+1])
+// (ascending), all next to cell seg_nbr[s]. One thread per segment keeps the sums in a fixed order.
+struct GhostSegments {
+    int n;
+    const int* ptr;
+    const int* nbr;
+    const int* ghost;
+};
+
+// Transpose of k_fill_ghosts on adjoint rows: the ghost row's adjoint moves to its interior neighbour
+// through (dG/du)^T, the part owed to the condition's value goes to vbar[j][k] (per ghost, summed per
+// condition by k_bc_value_reduce), and the ghost row is cleared (the fill overwrites the ghost's old
+// value, which therefore has no influence).
+template <int DIM, int NS>
+__global__ void __launch_bounds__(256) k_fill_ghosts_vjp(GhostBC G, GhostSegments S, double* __restrict__ Ub, double* __restrict__ vbar) {
+    using D = Dims<DIM, NS>;
+    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sidx >= S.n) return;
+    const int i = S.nbr[sidx];
+    double acc[D::NC];
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) acc[k] = 0.0;
+    for (int q = S.ptr[sidx]; q < S.ptr[sidx + 1]; q++) {
+        const int j = S.ghost[q];
+        const int g = G.cell[j];
+        const abl_bc bc = G.table[G.bc[j]];
+        double lg[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) {
+            lg[k] = Ub[(size_t)g * D::NC + k];
+            Ub[(size_t)g * D::NC + k] = 0.0;
+        }
+        double vb[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) vb[k] = 0.0;
+        switch (bc.kind) {
+            case ABL_BC_DIRICHLET:
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) {
+                    vb[k] = bc.enforce_at_face ? 2.0 * lg[k] : lg[k];
+                    if (bc.enforce_at_face) acc[k] -= lg[k];
+                }
+                break;
+            case ABL_BC_SLIP_WALL: {
+                // (I - 2 n n^T) is symmetric
+                double mn = 0;
+#pragma unroll
+                for (int d = 0; d < DIM; d++) mn += lg[2 + d] * G.normal[3 * (size_t)j + d];
+#pragma unroll
+                for (int d = 0; d < DIM; d++) lg[2 + d] -= 2.0 * mn * G.normal[3 * (size_t)j + d];
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) acc[k] += lg[k];
+                break;
+            }
+            case ABL_BC_NOSLIP_WALL:
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) acc[k] += (k >= 2 && k < 2 + DIM) ? -lg[k] : lg[k];
+                break;
+            default:
+#pragma unroll
+                for (int k = 0; k < D::NC; k++) acc[k] += lg[k];
+                break;
+        }
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) vbar[(size_t)j * D::NC + k] = vb[k];
+    }
+#pragma unroll
+    for (int k = 0; k < D::NC; k++) Ub[(size_t)i * D::NC + k] += acc[k];
+}
+
+// out[b][k] += sum over the ghosts j of condition b of vbar[j][k]; one block per condition, each thread a
+// fixed stride of ghosts, then a fixed-shape tree: the same sum on every run.
+template <int UNUSED = 0>
+__global__ void __launch_bounds__(256) k_bc_value_reduce(int n_ghost, const int* __restrict__ bc, int nc, const double* __restrict__ vbar,
+                                                         double* __restrict__ out) {
+    __shared__ double red[256];
+    const int b = blockIdx.x;
+    for (int k = 0; k < nc; k++) {
+        double acc = 0.0;
+        for (int j = threadIdx.x; j < n_ghost; j += blockDim.x)
+            if (bc[j] == b) acc += vbar[(size_t)j * nc + k];
+        red[threadIdx.x] = acc;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[(size_t)b * ABL_BC_MAX_COMPONENTS + k] += red[0];
+        __syncthreads();
+    }
+}
+
+// J = sum_j w_j p(U_{c_j}) over distinct cells c_j: per block a fixed-shape partial sum (the host adds
+// the partials in block order); with Ub, Ub[c_j] += w_j dp/dU (the reverse of the EOS decode).
+template <int DIM, int NS>
+__global__ void __launch_bounds__(256) k_pressure_functional(Phys P, int n, const int* __restrict__ cells, const double* __restrict__ w,
+                                                             const double* __restrict__ U, double* __restrict__ partial, double* __restrict__ Ub,
+                                                             int* status) {
+    using D = Dims<DIM, NS>;
+    __shared__ double red[256];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double val = 0.0;
+    if (j < n) {
+        const int c = cells[j];
+        double u[D::NC];
+        load_state<DIM, NS>(U, c, u);
+        bool ok = true;
+        const Decoded<double> dd = decode<DIM, NS>(P, NS, u, 300.0, &ok);
+        val = w[j] * dd.p;
+        if (!ok) atomicOr(status, kStatusEos);
+        if (Ub) {
+            double ub[D::NC];
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) ub[k] = 0.0;
+            decode_vjp<DIM, NS>(P, NS, u, dd, 0.0, 0.0, w[j], ub);
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) Ub[(size_t)c * D::NC + k] += ub[k];
+        }
+    }
+    red[threadIdx.x] = val;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
 
 }  // namespace abl

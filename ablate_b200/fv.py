@@ -314,6 +314,8 @@ class FiniteVolumeSolver:
         nc, na, ncell, nf = (C.c_int32() for _ in range(4))
         L.check(L.lib.abl_fv_sizes(h, C.byref(nc), C.byref(na), C.byref(ncell), C.byref(nf)))
         self.nc, self.naux, self.n_cells, self.n_faces = nc.value, na.value, ncell.value, nf.value
+        self._n_bc = 1  # every ghost is outflow until SetBoundary
+        self.device = device
 
     def RegisterRHSFunction(self, name: str, obj):
         self.registered.append(name)
@@ -369,14 +371,53 @@ class FiniteVolumeSolver:
         cb = None if cell_bc is None else np.ascontiguousarray(cell_bc, dtype=np.int32)
         L.check(L.lib.abl_fv_set_boundary(self.handle, len(table), C.cast(arr, C.c_void_p), L.iptr(cb) if cb is not None else None),
                 "abl_fv_set_boundary")
+        self._n_bc = len(table)
 
     def FillGhostsDevice(self, U_ptr: int, stream: int = 0):
         L.check(L.lib.abl_fv_fill_ghosts(self.handle, 0.0, C.c_void_p(U_ptr), C.c_void_p(stream)), "abl_fv_fill_ghosts")
+
+    def FillGhostsJVPDevice(self, dU_ptr: int, stream: int = 0):
+        """Tangent of the ghost fill on a perturbation (in place)."""
+        L.check(L.lib.abl_fv_fill_ghosts_jvp(self.handle, C.c_void_p(dU_ptr), C.c_void_p(stream)), "abl_fv_fill_ghosts_jvp")
+
+    def FillGhostsVJPDevice(self, Ubar_ptr: int, stream: int = 0) -> np.ndarray:
+        """Adjoint of the ghost fill on adjoint rows (in place); returns the adjoint of every condition's
+        value, shape (number of conditions, L.BC_MAX_COMPONENTS)."""
+        vb = np.zeros((self._n_bc, L.BC_MAX_COMPONENTS))
+        L.check(L.lib.abl_fv_fill_ghosts_vjp(self.handle, C.c_void_p(Ubar_ptr), vb.ctypes.data_as(C.c_void_p), C.c_void_p(stream)),
+                "abl_fv_fill_ghosts_vjp")
+        return vb
+
+    def SetPressureFunctional(self, cells, weights):
+        """J(U) = sum_j weights[j] p(U[cells[j]]); repeated cells are merged (their weights added)."""
+        cells = np.asarray(cells, dtype=np.int64)
+        weights = np.asarray(weights, dtype=np.float64)
+        uc, inv = np.unique(cells, return_inverse=True)
+        w = np.zeros(uc.size)
+        np.add.at(w, inv, weights)
+        c32 = np.ascontiguousarray(uc, dtype=np.int32)
+        L.check(L.lib.abl_fv_set_pressure_functional(self.handle, c32.size, L.iptr(c32), w.ctypes.data_as(C.c_void_p)),
+                "abl_fv_set_pressure_functional")
+
+    def PressureFunctionalDevice(self, U_ptr: int, Ubar_ptr: int = 0, stream: int = 0) -> float:
+        """J at the device state; with Ubar_ptr, dJ/dU is added into those rows."""
+        J = C.c_double(0.0)
+        L.check(L.lib.abl_fv_pressure_functional(self.handle, C.c_void_p(U_ptr), C.byref(J), C.c_void_p(Ubar_ptr or None),
+                                                 C.c_void_p(stream)), "abl_fv_pressure_functional")
+        return J.value
 
     def CflTimeStepDevice(self, U_ptr: int, cfl: float, stream: int = 0) -> float:
         dt = C.c_double(0.0)
         L.check(L.lib.abl_fv_cfl_dt(self.handle, C.c_void_p(U_ptr), float(cfl), C.byref(dt), C.c_void_p(stream)), "abl_fv_cfl_dt")
         return dt.value
+
+    def RkStageDevice(self, a: float, U0_ptr: int, b: float, Us_ptr: int, dt: float, F_ptr: int, Uout_ptr: int, stream: int = 0):
+        """Uout = a U0 + b (Us + dt F) on the owned rows (a == 0 drops U0)."""
+        L.check(L.lib.abl_fv_rk_stage(self.handle, float(a), C.c_void_p(U0_ptr or None), float(b), C.c_void_p(Us_ptr), float(dt),
+                                      C.c_void_p(F_ptr), C.c_void_p(Uout_ptr), C.c_void_p(stream)), "abl_fv_rk_stage")
+
+    def NormalizeSpeciesDevice(self, U_ptr: int, stream: int = 0):
+        L.check(L.lib.abl_fv_normalize_species(self.handle, C.c_void_p(U_ptr), C.c_void_p(stream)), "abl_fv_normalize_species")
 
     def StepDevice(self, scheme: int, time: float, dt: float, U_ptr: int, precision: int = L.PRECISION_FP64, stream: int = 0):
         L.check(L.lib.abl_fv_step(self.handle, scheme, time, dt, C.c_void_p(U_ptr), precision, C.c_void_p(stream)), "abl_fv_step")

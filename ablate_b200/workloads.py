@@ -37,6 +37,8 @@ class Workload:
     limiter: str
     U: np.ndarray  # (n_cells, nc) including ghost cells
     description: str
+    boundary: tuple | None = None    # (condition table, per-cell condition index) for SetBoundary
+    functional: tuple | None = None  # (cells, weights) of the wall-pressure functional
 
     def solver(self, device: int = 0) -> fv.FiniteVolumeSolver:
         return fv.FiniteVolumeSolver(self.mesh, self.eos, self.processes, self.petscfv_type, self.limiter, device=device)
@@ -233,6 +235,48 @@ def channel_tets(n: int = 2_000_000, ns: int = 9, seed: int = 20261205) -> Workl
     procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
     return Workload("channel_tets", mesh, eos, procs, "leastsquares", "vanleer", U,
                     f"3D {mesh.n_interior} seeded Delaunay tets in a 1x0.2x0.2 channel, {ns} NASA-7 species, AUSM+up + LSQ + van Leer, Le = 1")
+
+
+def wall3d(n: int = 128, seed: int = 20261206, speed_mach: float = 0.3, order: str = "morton") -> Workload:
+    """Wall-bounded variant of the Taylor-Green physics for the functional gradient: n^3 hex cells on
+    the unit cube, periodic in z, a Dirichlet inlet at x = 0 (uniform flow at Mach `speed_mach` along
+    x, T 300 K, p 101325 Pa), outflow at x = 1, no-slip walls at y = 0 and y = 1. Initial state: the
+    inlet flow with 0.5 % seeded white noise on the velocity and on the density. The functional is the
+    pressure integrated over the wall patch y = 0, 0.25 < x < 0.75 (the cells next to those wall faces,
+    weighted by the face area). AUSM+up + least squares + minmod, constant mu = 1.8e-5, Pr 0.72."""
+    from .adjoint import inlet_state
+    mesh = box_mesh((n, n, n), periodic=(False, False, True), order=order)
+    rng = np.random.default_rng(seed)
+    gamma, R, T0, p0 = 1.4, 287.0, 300.0, 101325.0
+    rho0 = p0 / (R * T0)
+    V = speed_mach * np.sqrt(gamma * R * T0)
+    nc = mesh.n_cells
+    rho = rho0 * (1.0 + 0.005 * rng.standard_normal(nc))
+    vel = np.zeros((nc, 3))
+    vel[:, 0] = V
+    vel += 0.005 * V * rng.standard_normal((nc, 3))
+    U = np.zeros((nc, 5))
+    U[:, 0] = rho
+    U[:, 2:5] = rho[:, None] * vel
+    U[:, 1] = p0 / (gamma - 1.0) + 0.5 * rho * (vel ** 2).sum(1)
+    inlet, _ = inlet_state(rho0, p0, V, (1.0, 0.0, 0.0), gamma)
+    table = [(L.BC_DIRICHLET, list(inlet), False), (L.BC_OUTFLOW, None, False), (L.BC_NOSLIP_WALL, None, False)]
+    cell_bc = np.zeros(nc, np.int32)
+    ghosts = np.nonzero(mesh.cell_kind == L.CELL_BOUNDARY)[0]
+    gx, gy = mesh.cell_centroid[ghosts, 0], mesh.cell_centroid[ghosts, 1]
+    cell_bc[ghosts] = np.where(gx < 0.0, 0, np.where(gx > 1.0, 1, 2))
+    inner = ghost_interior_map(mesh)
+    patch = (gy < 0.0) & (gx > 0.25) & (gx < 0.75)
+    area = 1.0 / n ** 2
+    fill_outflow_ghosts(mesh, U)
+    mu, pr = 1.8e-5, 0.72
+    cp = gamma * R / (gamma - 1.0)
+    eos = fv.PerfectGas({"gamma": gamma, "Rgas": R})
+    procs = [fv.NavierStokesTransport({"cfl": 0.5}, eos, fv.AusmpUp(0.3), fv.Constant(k=mu * cp / pr, mu=mu))]
+    return Workload("wall3d", mesh, eos, procs, "leastsquares", "minmod", U,
+                    f"3D NS {n}^3 hex channel: Dirichlet inlet M{speed_mach} at x=0, outflow x=1, no-slip walls y=0,1, periodic z; "
+                    "AUSM+up + LSQ + minmod, mu 1.8e-5, Pr 0.72; functional: pressure integrated over the wall patch y=0, 0.25<x<0.75",
+                    boundary=(table, cell_bc), functional=(inner[patch], np.full(int(patch.sum()), area)))
 
 
 def initial_aux(w: Workload) -> np.ndarray:

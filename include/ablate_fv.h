@@ -272,6 +272,27 @@ int abl_fv_set_boundary(abl_fv* fv, int32_t n_bc, const abl_bc* table, const int
 /* Fill the ghost rows of U_dev from their interior neighbours (before every RHS evaluation). */
 int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream);
 
+/* Tangent of the fill on a perturbation dU_dev (in place): every ghost row becomes dG/du times its
+ * interior neighbour's row (the condition values are constants: a plain Dirichlet ghost gets 0). */
+int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream);
+
+/* Adjoint of the fill on adjoint rows Ubar_dev (in place): each ghost row's adjoint is added to its
+ * interior neighbour through (dG/du)^T and the ghost row is cleared; value_bar_host[n_bc][16] (may be
+ * NULL) accumulates the adjoint of every condition's value[] (ABL_BC_DIRICHLET only; the other kinds
+ * take no value). Sums run in a fixed order: the same inputs give the same bits. With abl_fv_vjp and
+ * abl_fv_rk_stage this is the reverse of abl_fv_step, for gradients of a functional of the marched state
+ * with respect to the initial state and the boundary values. No reference counterpart: the reference
+ * has no adjoint of its boundary conditions. */
+int abl_fv_fill_ghosts_vjp(abl_fv* fv, double* Ubar_dev, double* value_bar_host, void* stream);
+
+/* Pressure functional J(U) = sum_j w_j p(U_{c_j}) over distinct cells c_j (for the pressure integrated
+ * over a wall patch: the cells next to the wall faces, w = face area; a no-slip ghost mirrors only the
+ * momentum, so the wall-face pressure is the cell's). set_ registers the cells and weights (host
+ * arrays, validated: in range, no cell twice). The evaluation returns J in *J_host and, when Ubar_dev
+ * is not NULL, adds w_j dp/dU into Ubar_dev's rows (the reverse of the EOS decode, NASA-7 included). */
+int abl_fv_set_pressure_functional(abl_fv* fv, int32_t n, const int32_t* cells, const double* weights);
+int abl_fv_pressure_functional(abl_fv* fv, const double* U_dev, double* J_host, double* Ubar_dev, void* stream);
+
 /* CFL time step of NavierStokesTransport::ComputeCflTimeStep (navierStokesTransport.cpp:209-278):
  * min over owned cells of cfl * 2 r_min / (a / alpha + sum_d |u_d|), r_min the smallest cell-centroid to
  * face-centroid distance, a the speed of sound at T(U) (guess 300 K), alpha the pressure-gradient

@@ -9,6 +9,12 @@ path; the product runs these steps as CUDA kernels (ablate_b200/csrc/fv_step.cuh
   cfl_dt             NavierStokesTransport::ComputeCflTimeStep (navierStokesTransport.cpp:209-278) with the
                      minimum cell radius of FiniteVolumeSolver (finiteVolumeSolver.cpp:172-218)
   normalize_species  SpeciesTransport::NormalizeSpecies (speciesTransport.cpp:343-403)
+  fill_ghosts_tangent, fill_ghosts_adjoint
+                     derivative of the ghost fill and its transpose (no reference counterpart: the
+                     reference has no adjoint); the transpose sums per interior cell in ascending ghost order
+  pressure_functional  J = sum_j w_j p(U_c_j) and, for a perfect gas, dJ/dU in closed form
+                     (p = (gamma - 1)(rho E - |rho u|^2 / (2 rho)), src/eos/perfectGas.cpp:49-197)
+  march_functional   J after a fixed-step march (for finite differences of the marched functional)
   euler_step, ssprk3_step, integrate
                      explicit steps; integrate chooses steps as AdaptPhysics does (the CFL step times
                      the safety factor, src/solver/adaptPhysics.cpp:3-24) and ends exactly at the final
@@ -57,6 +63,85 @@ def fill_ghosts(mesh, U, table, cell_bc=None):
             u[2:2 + dim] = -u[2:2 + dim]
         U[g] = u
     return U
+
+
+def fill_ghosts_tangent(mesh, dU, table, cell_bc=None):
+    """Derivative of fill_ghosts with respect to the interior rows (the condition values held fixed)."""
+    ghosts, inner, normal = ghost_pairs(mesh)
+    dim = mesh.dim
+    for j in range(ghosts.size):
+        g, i = ghosts[j], inner[j]
+        kind, value, enforce = table[0 if cell_bc is None else cell_bc[g]]
+        u = dU[i].copy()
+        if kind == DIRICHLET:
+            u = -u if enforce else np.zeros_like(u)
+        elif kind == SLIP_WALL:
+            mn = float(np.dot(u[2:2 + dim], normal[j, :dim]))
+            u[2:2 + dim] -= 2.0 * mn * normal[j, :dim]
+        elif kind == NOSLIP_WALL:
+            u[2:2 + dim] = -u[2:2 + dim]
+        dU[g] = u
+    return dU
+
+
+def fill_ghosts_adjoint(mesh, Ub, table, cell_bc=None):
+    """Transpose of fill_ghosts on adjoint rows, in place: returns (Ub, vbar[n_bc][nc]). Per interior cell
+    the ghosts' terms are summed in ascending ghost order first, then added to the cell's row."""
+    ghosts, inner, normal = ghost_pairs(mesh)
+    dim = mesh.dim
+    nc = Ub.shape[1]
+    vbar = np.zeros((len(table), nc))
+    acc = {}
+    for j in np.lexsort((ghosts, inner)):
+        g, i = ghosts[j], inner[j]
+        b = 0 if cell_bc is None else cell_bc[g]
+        kind, value, enforce = table[b]
+        lg = Ub[g].copy()
+        Ub[g] = 0.0
+        a = acc.setdefault(i, np.zeros(nc))
+        if kind == DIRICHLET:
+            vbar[b] += 2.0 * lg if enforce else lg
+            if enforce:
+                a -= lg
+        elif kind == SLIP_WALL:
+            mn = float(np.dot(lg[2:2 + dim], normal[j, :dim]))
+            lg[2:2 + dim] -= 2.0 * mn * normal[j, :dim]
+            a += lg
+        elif kind == NOSLIP_WALL:
+            lg[2:2 + dim] = -lg[2:2 + dim]
+            a += lg
+        else:
+            a += lg
+    for i, a in acc.items():
+        Ub[i] += a
+    return Ub, vbar
+
+
+def pressure_functional(mesh, physics, U, cells, weights, gamma=None):
+    """J = sum_j w_j p(U[c_j]) through the oracle EOS; with gamma (perfect gas), also dJ/dU."""
+    Uc = np.ascontiguousarray(U[cells])
+    T = orc.eos(physics, mesh.dim, L.PROP_TEMPERATURE, Uc, np.full(len(cells), 300.0))[:, 0]
+    p = orc.eos(physics, mesh.dim, L.PROP_PRESSURE, Uc, T)[:, 0]
+    J = float(np.dot(weights, p))
+    if gamma is None:
+        return J, None
+    G = np.zeros_like(U)
+    rho = Uc[:, 0]
+    vel = Uc[:, 2:2 + mesh.dim] / rho[:, None]
+    G[cells, 0] = weights * (gamma - 1.0) * 0.5 * (vel ** 2).sum(1)
+    G[cells, 1] = weights * (gamma - 1.0)
+    G[cells, 2:2 + mesh.dim] = -(weights * (gamma - 1.0))[:, None] * vel
+    return J, G
+
+
+def march_functional(mesh, physics, U, dt, n_steps, table, cell_bc, cells, weights, step="ssprk3"):
+    """J after n_steps fixed steps of size dt from U (the march the device adjoint differentiates)."""
+    U = U.copy()
+    for _ in range(n_steps):
+        U = euler_step(mesh, physics, U, dt, table, cell_bc) if step == "euler" else ssprk3_step(mesh, physics, U, dt, table, cell_bc)
+        if step == "euler":
+            fill_ghosts(mesh, U, table, cell_bc)
+    return pressure_functional(mesh, physics, U, cells, weights)[0]
 
 
 def min_cell_radius(mesh):
