@@ -37,6 +37,7 @@ CELL_OWNED, CELL_BOUNDARY, CELL_HALO, CELL_HALO_OUTER = range(4)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 BC_OUTFLOW, BC_DIRICHLET, BC_SLIP_WALL, BC_NOSLIP_WALL = range(4)
 BC_MAX_COMPONENTS = 16
+JVP_EXACT, JVP_FROZEN_LIMITER = 0, 1
 STEP_EULER, STEP_SSPRK3 = 0, 1
 RHS_OVERWRITE = 0x100
 
@@ -97,6 +98,7 @@ SIGNATURES = {
     "abl_fv_set_boundary": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, _ip]),
     "abl_fv_fill_ghosts": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
     "abl_fv_fill_ghosts_jvp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "abl_fv_set_jvp_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "abl_fv_fill_ghosts_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_set_pressure_functional": (C.c_int, [C.c_void_p, C.c_int32, _ip, C.c_void_p]),
     "abl_fv_pressure_functional": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p, C.c_void_p]),

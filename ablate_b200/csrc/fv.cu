@@ -992,6 +992,14 @@ int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream) {
     });
 }
 
+int abl_fv_set_jvp_mode(abl_fv* fv, int mode) {
+    return guarded([&] {
+        if (!fv) throw std::invalid_argument("abl_fv_set_jvp_mode: NULL handle");
+        if (mode != ABL_JVP_EXACT && mode != ABL_JVP_FROZEN_LIMITER) throw std::invalid_argument("abl_fv_set_jvp_mode: unknown mode");
+        fv->phys.jvp_frozen_limiter = mode == ABL_JVP_FROZEN_LIMITER;
+    });
+}
+
 int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream) {
     return guarded([&] {
         if (!fv || !dU_dev) throw std::invalid_argument("abl_fv_fill_ghosts_jvp: NULL argument");

@@ -282,6 +282,12 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
             }
         }
     }
+    if constexpr (std::is_same<G, Dual>::value) {
+        if (P.jvp_frozen_limiter) {
+#pragma unroll
+            for (int k = 0; k < D::NC; k++) phi[k].d = 0.0;
+        }
+    }
     bool cancel = false;
 #pragma unroll
     for (int k = 0; k < D::NC; k++) {

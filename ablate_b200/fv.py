@@ -345,6 +345,10 @@ class FiniteVolumeSolver:
         L.check(L.lib.abl_fv_jvp(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(dU_ptr), C.c_void_p(F_ptr or None), C.c_void_p(dF_ptr),
                                  C.c_void_p(stream)), "abl_fv_jvp")
 
+    def SetJVPMode(self, mode: int):
+        """L.JVP_EXACT (default) or L.JVP_FROZEN_LIMITER for the following JVP calls."""
+        L.check(L.lib.abl_fv_set_jvp_mode(self.handle, int(mode)), "abl_fv_set_jvp_mode")
+
     def ComputeVJP(self, time: float, locX: np.ndarray, Fbar: np.ndarray, Ubar: np.ndarray):
         """Ubar += J(locX)^T Fbar, host arrays (n_cells, nc); Fbar is read on owned cells."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

@@ -152,17 +152,65 @@ def read_traffic(workload: str, precision: str, kernel: str, n_cells: int):
     return None
 
 
-def wall_studies(w, solver, U, stream, dev, K=10, horizon=16):
+def implicit_vs_explicit(solver, U0, owned, dt_e, horizon, stream, dev, ms_of):
+    """BDF2 (Newton-GMRES(30) on the JVP, frozen-limiter tangent) at 1, 2, 4 and 8 times the CFL-0.5
+    step against SSP-RK3 at that step, both measured against SSP-RK3 at 1/8 of it over `horizon` steps."""
+    import torch
+    from ablate_b200 import _lib as L
+    from ablate_b200.implicit import BDFStepper
+
+    st = stream.cuda_stream
+
+    def ssprk3(dt, n):
+        Ux = U0.clone()
+        for _ in range(n):
+            solver.StepDevice(L.STEP_SSPRK3, 0.0, dt, Ux.data_ptr(), L.PRECISION_FP64, st)
+        return Ux
+
+    U_ref, ref_ms = ms_of(lambda: ssprk3(dt_e / 8, horizon * 8))
+    scale = float((U_ref[owned] - U0[owned]).norm())
+
+    def err(X):
+        return float((X[owned] - U_ref[owned]).norm()) / scale
+
+    U_ex, ex_ms = ms_of(lambda: ssprk3(dt_e, horizon))
+    rows = [{"method": "ssprk3", "dt_over_cfl05": 1, "steps": horizon, "ms": ex_ms, "rel_error": err(U_ex)}]
+    for m in (1, 2, 4, 8):
+        bdf = BDFStepper(solver, m * dt_e)
+
+        def run():
+            Ux = U0.clone()
+            for _ in range(horizon // m):
+                bdf.step(Ux)
+            return Ux
+
+        U_im, im_ms = ms_of(run)
+        rows.append({"method": "bdf2", "dt_over_cfl05": m, "steps": horizon // m, "ms": im_ms, "rel_error": err(U_im),
+                     "newton": bdf.stats["newton"], "gmres_iterations": bdf.stats["gmres"], "jvp": bdf.stats["jvp"], "rhs": bdf.stats["rhs"],
+                     "gmres_unconverged": bdf.stats["ksp_unconverged"], "newton_unconverged": bdf.stats["snes_unconverged"],
+                     "newton_residual_reduction": [float(r) for r in bdf.reductions]})
+    if solver.Status() != L.OK:
+        raise RuntimeError("device status after the implicit/explicit comparison")
+    ex_err = rows[0]["rel_error"]
+    matched = [r for r in rows[1:] if r["rel_error"] <= ex_err]
+    verdict = (f"BDF2 at {matched[-1]['dt_over_cfl05']}x the explicit step matches its accuracy in {matched[-1]['ms']:.1f} ms vs {ex_ms:.1f} ms"
+               if matched else
+               f"no BDF2 step size reaches the explicit error {ex_err:.2e}; the smallest BDF2 error is "
+               f"{min(r['rel_error'] for r in rows[1:]):.2e}")
+    return {"reference": f"ssprk3 at dt/8 ({horizon * 8} steps, {ref_ms:.1f} ms)", "runs": rows, "equal_accuracy": verdict}
+
+
+def wall_studies(w, solver, U, stream, dev, K=10, horizon=8):
     """The wall-bounded channel's two uses of the derivatives, on the device:
     (1) the gradient of the wall-patch pressure after K SSP-RK3 steps (fixed step, half the CFL-1 step)
         with respect to the initial state and the inlet speed: forward march with checkpoints, then
         the adjoint march (VJP per stage + transposed ghost fill);
-    (2) BDF2 with Newton-GMRES(30) on the JVP against SSP-RK3 at CFL 0.5, both measured against an
-        SSP-RK3 march at 1/8 of that step over `horizon` CFL-0.5 steps: error and device time."""
+    (2) BDF2 with Newton-GMRES(30) on the JVP against SSP-RK3 at CFL 0.5, with the configured minmod
+        limiter and with unlimited gradients (a differentiable residual)."""
     import torch
     from ablate_b200 import _lib as L
+    from ablate_b200 import fv
     from ablate_b200.adjoint import ExplicitMarch, functional_gradient, inlet_state
-    from ablate_b200.implicit import BDFStepper
 
     st = stream.cuda_stream
     table, cell_bc = w.boundary
@@ -172,7 +220,7 @@ def wall_studies(w, solver, U, stream, dev, K=10, horizon=16):
     solver.FillGhostsDevice(U0.data_ptr(), st)
     dt_e = solver.CflTimeStepDevice(U0.data_ptr(), 0.5, st)
 
-    def ev_ms(fn):
+    def ms_of(fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(dev)
         a.record(stream)
@@ -183,10 +231,10 @@ def wall_studies(w, solver, U, stream, dev, K=10, horizon=16):
 
     march = ExplicitMarch(solver, L.STEP_SSPRK3, dt_e, K)
     functional_gradient(solver, march, U0)  # warm-up
-    UK, fwd_ms = ev_ms(lambda: march.forward(U0, keep=True))
+    UK, fwd_ms = ms_of(lambda: march.forward(U0, keep=True))
     lam = torch.zeros_like(UK)
     J = solver.PressureFunctionalDevice(UK.data_ptr(), lam.data_ptr(), st)
-    (lam0, vbar), adj_ms = ev_ms(lambda: march.adjoint(lam))
+    (lam0, vbar), adj_ms = ms_of(lambda: march.adjoint(lam))
     if solver.Status() != L.OK:
         raise RuntimeError("device status after the functional gradient")
     rho0, p0 = 101325.0 / (287.0 * 300.0), 101325.0
@@ -198,45 +246,15 @@ def wall_studies(w, solver, U, stream, dev, K=10, horizon=16):
                     "central differences in the tests"}
 
     owned = torch.from_numpy(w.mesh.cell_kind == L.CELL_OWNED).to(dev)
-    T_end = horizon * dt_e
-
-    def ssprk3(dt, n):
-        Ux = U0.clone()
-        for _ in range(n):
-            solver.StepDevice(L.STEP_SSPRK3, 0.0, dt, Ux.data_ptr(), L.PRECISION_FP64, st)
-        return Ux
-
-    U_ref, ref_ms = ev_ms(lambda: ssprk3(dt_e / 8, horizon * 8))
-    scale = float((U_ref[owned] - U0[owned]).norm())
-
-    def err(X):
-        return float((X[owned] - U_ref[owned]).norm()) / scale
-
-    U_ex, ex_ms = ev_ms(lambda: ssprk3(dt_e, horizon))
-    rows = [{"method": "ssprk3", "dt_over_cfl05": 1, "steps": horizon, "ms": ex_ms, "rel_error": err(U_ex)}]
-    for m in (1, 2, 4, 8):
-        bdf = BDFStepper(solver, m * dt_e)
-
-        def run():
-            Ux = U0.clone()
-            for _ in range(horizon // m):
-                bdf.step(Ux)
-            return Ux
-
-        U_im, im_ms = ev_ms(run)
-        rows.append({"method": "bdf2 newton-gmres(30) on the jvp", "dt_over_cfl05": m, "steps": horizon // m, "ms": im_ms,
-                     "rel_error": err(U_im), "newton": bdf.stats["newton"], "gmres_iterations": bdf.stats["gmres"],
-                     "jvp": bdf.stats["jvp"], "rhs": bdf.stats["rhs"]})
-    if solver.Status() != L.OK:
-        raise RuntimeError("device status after the implicit/explicit comparison")
-    ex_err = rows[0]["rel_error"]
-    matched = [r for r in rows[1:] if r["rel_error"] <= ex_err]
-    verdict = (f"BDF2 at {matched[-1]['dt_over_cfl05']}x the explicit step matches its accuracy in {matched[-1]['ms']:.1f} ms vs {ex_ms:.1f} ms"
-               if matched else
-               f"no BDF2 step size reaches the explicit error {ex_err:.2e}; the smallest BDF2 error is "
-               f"{min(r['rel_error'] for r in rows[1:]):.2e}")
-    comp = {"t_end": T_end, "reference": f"ssprk3 at dt/8 ({horizon * 8} steps, {ref_ms:.1f} ms)", "runs": rows, "equal_accuracy": verdict,
-            "note": "rel_error = |U - U_ref| / |U_ref - U_0| over the owned cells; device time with CUDA events around each march"}
+    comp = {"t_end": horizon * dt_e, "horizon_steps": horizon,
+            "minmod": implicit_vs_explicit(solver, U0, owned, dt_e, horizon, stream, dev, ms_of)}
+    unlimited = fv.FiniteVolumeSolver(w.mesh, w.eos, w.processes, w.petscfv_type, "none", device=solver.device)
+    unlimited.SetBoundary(table, cell_bc)
+    comp["unlimited"] = implicit_vs_explicit(unlimited, U0, owned, dt_e, horizon, stream, dev, ms_of)
+    unlimited.close()
+    comp["note"] = ("rel_error = |U - U_ref| / |U_ref - U_0| over the owned cells; device time with CUDA events around each march; "
+                    "Newton: SNES defaults (rtol 1e-8, stol 1e-8) capped at 10 iterations with a backtracking line search, "
+                    "GMRES(30) at rtol 1e-5 capped at 300 iterations, state scaled per component")
     return grad, comp
 
 

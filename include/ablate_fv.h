@@ -189,6 +189,15 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
  * theorem on e_s(T, Y) = e. The reference's counterpart is PETSc's finite-difference Jacobian-vector
  * product through the same RHS (MatMFFD on TSComputeRHSFunction). */
 int abl_fv_jvp(abl_fv* fv, double time, const double* U_dev, const double* dU_dev, double* F_dev, double* dF_dev, void* stream);
+
+/* Tangent mode of the following abl_fv_jvp calls. ABL_JVP_EXACT (the default) differentiates every
+ * branch it takes, the limiter factor included. ABL_JVP_FROZEN_LIMITER holds each limiter factor at
+ * its value (its derivative, which carries 1/(grad . dx) terms and jumps where the minimising face
+ * changes, is dropped): the Jacobian a matrix-free Newton-Krylov step uses to stay well conditioned on
+ * limited schemes. abl_fv_vjp is the transpose of the exact tangent in either mode. */
+#define ABL_JVP_EXACT 0
+#define ABL_JVP_FROZEN_LIMITER 1
+int abl_fv_set_jvp_mode(abl_fv* fv, int mode);
 int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double* dU_host, double* F_host, double* dF_host);
 
 /* Adjoint (vector-Jacobian product) of abl_fv_rhs at FP64: Ubar += J(U)^T Fbar. Fbar is read on owned

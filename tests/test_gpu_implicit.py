@@ -1,5 +1,8 @@
 """Matrix-free BDF1/BDF2 with Newton-GMRES(30) on the device JVP (ablate_b200.implicit): the step solves
-its nonlinear system, and BDF2 converges at second order against a fine SSP-RK3 march."""
+its nonlinear system, and BDF2 converges at second order against a fine SSP-RK3 march. These run the
+wall-bounded channel with unlimited least-squares gradients: Newton needs a differentiable residual, and
+a limited scheme is not (the limiter's branches and the minimising face switch under the Newton
+updates; the bench reports how far Newton gets there)."""
 import numpy as np
 import pytest
 
@@ -13,11 +16,41 @@ pytestmark = pytest.mark.gpu
 
 def _setup(n=10):
     w = workloads.wall3d(n)
+    w.limiter = "none"
     phys, keep = w.physics()
     s = w.solver()
     s.SetBoundary(*w.boundary)
     dt = 0.5 * S.cfl_dt(w.mesh, phys, w.U, 1.0)
     return w, s, dt
+
+
+@pytest.mark.parametrize("name", ["tgv3d_ausmpup_lsq_minmod_visc", "box2d_ausmpup_vanleer_suth"])
+def test_frozen_limiter_tangent(name):
+    """The frozen-limiter tangent is linear in the direction, differs from the exact one only through
+    the limiter factor's derivative, and leaves the exact mode (and the VJP) untouched."""
+    torch = pytest.importorskip("torch")
+    from tests import rhs_cases as R
+    w = R.case(name)
+    s = w.solver()
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream().cuda_stream
+    rng = np.random.default_rng(3)
+    U = torch.from_numpy(w.U).to(dev)
+    a = torch.from_numpy(rng.standard_normal(w.U.shape) * np.abs(w.U).mean(0)).to(dev)
+    b = torch.from_numpy(rng.standard_normal(w.U.shape) * np.abs(w.U).mean(0)).to(dev)
+
+    def jvp(v):
+        dF = torch.zeros_like(U)
+        s.ComputeJVPDevice(0.0, U.data_ptr(), v.data_ptr(), dF.data_ptr(), 0, st)
+        return dF
+
+    exact = jvp(a)
+    s.SetJVPMode(L.JVP_FROZEN_LIMITER)
+    fa, fb, fab = jvp(a), jvp(b), jvp(2.0 * a - 3.0 * b)
+    s.SetJVPMode(L.JVP_EXACT)
+    assert torch.equal(jvp(a), exact)
+    assert float((fab - (2.0 * fa - 3.0 * fb)).norm()) <= 1e-12 * float(fab.norm())
+    assert float((fa - exact).norm()) > 1e-6 * float(exact.norm())  # the limiter is active here
 
 
 def test_bdf_steps_solve_their_nonlinear_system():
@@ -53,17 +86,19 @@ def test_bdf2_is_second_order():
     U0 = torch.from_numpy(w.U).to(dev)
     s.FillGhostsDevice(U0.data_ptr(), st)
     owned = torch.from_numpy(w.mesh.cell_kind == L.CELL_OWNED).to(dev)
-    n = 8
+    n = 4  # march over 4 CFL-0.5 steps, at 1/2, 1/4 and 1/8 of that step
     ref = U0.clone()
-    for _ in range(n * 16):
-        s.StepDevice(L.STEP_SSPRK3, 0.0, dt / 16, ref.data_ptr(), L.PRECISION_FP64, st)
+    for _ in range(n * 64):
+        s.StepDevice(L.STEP_SSPRK3, 0.0, dt / 64, ref.data_ptr(), L.PRECISION_FP64, st)
     errs = []
-    for m in (1, 2):
+    for m in (2, 4, 8):
         bdf = BDFStepper(s, dt / m, snes_rtol=1e-10, ksp_rtol=1e-8)
         X = U0.clone()
         for _ in range(n * m):
             bdf.step(X)
         errs.append(float((X[owned] - ref[owned]).norm()))
+        assert bdf.stats["snes_unconverged"] == 0
     assert s.Status() == L.OK
-    order = np.log2(errs[0] / errs[1])
-    assert 1.6 <= order <= 2.6, (errs, order)
+    orders = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    # the BDF1 start adds a second-order term with a large constant: the order approaches 2 from below
+    assert orders[-1] >= 1.75 and orders[-1] <= 2.3 and orders[-1] >= orders[0] - 0.05, (errs, orders)

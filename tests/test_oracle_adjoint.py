@@ -66,6 +66,6 @@ def test_wall_workload_layout():
     assert np.all(cell_bc[g][x < 0] == 0) and np.all(cell_bc[g][x > 1] == 1)
     assert np.all(cell_bc[g][(y < 0) | (y > 1)] == 2)
     cells, wts = w.functional
-    assert cells.size == 4 * 8 and np.unique(cells).size == cells.size
-    assert np.all(w.mesh.cell_centroid[cells, 1] < 1.0 / 8)
-    assert np.isclose(wts.sum(), 0.5)  # half of the unit-length wall, unit depth
+    assert cells.size == 2 * 8 and np.unique(cells).size == cells.size
+    assert np.all(w.mesh.cell_centroid[cells, 1] < 1.0 / 8) and np.all(w.mesh.cell_centroid[cells, 0] < 0.25)
+    assert np.isclose(wts.sum(), 0.25)  # a quarter of the unit-length wall, unit depth
