@@ -635,6 +635,7 @@ struct AdjRow {
     using D = Dims<DIM, NS>;
     static constexpr int U = 0, G = D::NC, A = D::NC + D::NC * DIM, GA = D::NC + D::NC * DIM + D::NA;
     static constexpr int N = GA + D::NA * DIM;
+    static constexpr int S = N | 1;  // shared-memory row stride: odd, so rows of random cells spread over the banks
 };
 
 // one face backwards, this lane's side: the adjoint contributions are added into the side's
@@ -858,19 +859,21 @@ __global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
                                                                           const double* __restrict__ Fb, GradRec rec, AdjOut<DIM, NS> out,
                                                                           double* __restrict__ nbrec, int do_state, int do_aux, int* status) {
     using AR = AdjRow<DIM, NS>;
-    extern __shared__ double sacc[];  // [tile cells][AR::N]
+    extern __shared__ double sacc[];  // [tile cells][AR::S]
     const int t = blockIdx.x;
     const int cb = M.tile_cell_ptr[t], nct = M.tile_cell_ptr[t + 1] - cb;
-    for (int i = threadIdx.x; i < nct * AR::N; i += blockDim.x) sacc[i] = 0.0;
+    for (int i = threadIdx.x; i < nct * AR::S; i += blockDim.x) sacc[i] = 0.0;
     __syncthreads();
     bool ok = true, rok = true;
     const int side = threadIdx.x & 1, pair = threadIdx.x >> 1;
     const int base = M.col_base[t], ncol = M.col_base[t + 1] - base - 1;
+    const int fb = M.tile_face_ptr[t];
     for (int q = 0; q < ncol; q++) {
-        const int i = M.col_start[base + q] + pair;
-        const bool act = i < M.col_start[base + q + 1];
+        const int qa = M.col_start[base + q] + pair;
+        const bool act = qa < M.col_start[base + q + 1];
         const unsigned mask = __ballot_sync(0xffffffffu, act);  // both lanes of a face share act
         if (act) {
+            const int i = fb + M.tf_adj[qa];  // the face record
             const int2 lr = M.tf_cells[i];
             const int me = side ? lr.y : lr.x;
             double normal[DIM], fdxo[3];
@@ -884,7 +887,7 @@ __global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
             const int nb = M.tf_nb[i];
             double* dst = nullptr;
             if (slot != 0xffff)
-                dst = sacc + (size_t)slot * AR::N;
+                dst = sacc + (size_t)slot * AR::S;
             else if (nb >= 0 && M.kind[me] != ABL_CELL_OWNED)
                 dst = nbrec + (size_t)nb * AR::N;
             face_vjp_side<DIM, NS, FK>(M, P, mask, side, me, normal, fdxo, U, aux, grad, agrad, Fb, dst, &ok, &rok);
@@ -892,7 +895,7 @@ __global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
         __syncthreads();
     }
     for (int j = threadIdx.x; j < nct; j += blockDim.x)
-        cell_vjp<DIM, NS, LIM>(M, P, M.tile_cells[cb + j], U, sacc + (size_t)j * AR::N, rec, out, do_state, do_aux);
+        cell_vjp<DIM, NS, LIM>(M, P, M.tile_cells[cb + j], U, sacc + (size_t)j * AR::S, rec, out, do_state, do_aux);
     if (!ok) atomicOr(status, kStatusEos);
     if (!rok) atomicOr(status, kStatusRiemann);
 }

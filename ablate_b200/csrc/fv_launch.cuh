@@ -132,7 +132,7 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
     mark(fv, "k_tile_adjoint", s);
     if (fv->n_nb > 0) ABL_CUDA(cudaMemsetAsync(fv->adj_nb.p, 0, (size_t)fv->n_nb * AR::N * sizeof(double), s));
     if (M.n_tiles > 0) {
-        const size_t smem = (size_t)fv->tile_max_cells * AR::N * sizeof(double);
+        const size_t smem = (size_t)fv->tile_max_cells * AR::S * sizeof(double);
         if (smem > 227 * 1024) throw AblError(ABL_ERR_UNSUPPORTED, "adjoint accumulators exceed shared memory for this species count");
         // flux calculator and limiter fixed at compile time where a specialised kernel exists
         auto kern = k_tile_adjoint<DIM, NS, -1, -1>;

@@ -205,9 +205,11 @@ struct Tiles {
     std::vector<int32_t> tc_fptr;         // [n_owned+1] per tile cell into tc_face
     std::vector<uint16_t> tc_face;        // local face index | side << 15
     std::vector<uint32_t> tf_slot;        // [ntf] tile-local slot of L | of R << 16 (0xffff: not a tile cell)
+    std::vector<uint16_t> tf_fwd;         // [ntf] per tile, the record position of its k-th face in global order
+    std::vector<uint16_t> tf_adj;         // [ntf] per tile, the record position of its k-th face in adjoint colour order
     std::vector<int32_t> tf_nb;           // [ntf] record of the non-owned side, -1 if both sides are owned
     std::vector<int32_t> col_base;        // [n_tiles+1] into col_start
-    std::vector<int32_t> col_start;       // per tile: first tile face of each colour, then the end
+    std::vector<int32_t> col_start;       // per tile: first position (in tf_adj) of each adjoint colour, then the end
     std::vector<int32_t> face_nb;         // [n_faces] record index of faces with a non-owned side, else -1
     int n_nb = 0;                         // number of such records
     int max_colors = 0;
@@ -279,8 +281,8 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         if (faces.size() > 0x7fff) throw std::invalid_argument("tile has too many faces");
         t.max_faces = std::max(t.max_faces, (int)faces.size());
         lists.assign(ce - cb, {});
-        // greedy colouring over the tile cells each face touches, at most kColorCap faces per colour
-        // (one face per thread of the adjoint kernel's CTA, so every colour is one pass)
+        // first-fit colouring over the tile cells each face touches, at most kColorCap faces per colour:
+        // it orders the face records
         used.assign(ce - cb, 0);
         color.assign(faces.size(), 0);
         count.assign(64, 0);
@@ -298,7 +300,8 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             if (lL >= 0) used[lL] |= 1ull << c;
             if (lR >= 0) used[lR] |= 1ull << c;
         }
-        t.max_colors = std::max(t.max_colors, ncol);
+        (void)ncol;
+        // records in first-fit colour order (the order the mixed-precision flux pass reads fastest)
         order.resize(faces.size());
         for (size_t i = 0; i < faces.size(); i++) order[i] = (int)i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return color[a] < color[b]; });
@@ -307,7 +310,6 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         for (size_t q = 0; q < order.size(); q++) {
             const int i = order[q];
             pos[i] = (int)q;
-            if (q == 0 || color[order[q - 1]] != color[i]) t.col_start.push_back(base + (int)q);
             const int f = faces[i];
             const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
             t.tf_cells.push_back(L);
@@ -316,6 +318,44 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             for (int z = 0; z < 6; z++) t.tf_fdx.push_back(h.fdx[6 * (size_t)f + z]);
             t.tf_slot.push_back((uint32_t)(local[L] >= 0 ? local[L] : 0xffff) | ((uint32_t)(local[R] >= 0 ? local[R] : 0xffff) << 16));
             t.tf_nb.push_back(t.face_nb[f]);
+        }
+        for (size_t i = 0; i < faces.size(); i++) t.tf_fwd.push_back((uint16_t)pos[i]);
+        // the adjoint's colouring: balanced greedy. With K colours allowed each face takes the
+        // least-filled colour free at both its cells; K starts at the bound ceil(faces / kColorCap) and
+        // grows until every face fits. On an 8x8x4 hex tile (896 faces) that is 8 passes of 112 faces
+        // where first-fit needs 12 (six of them part-empty), and every pass ends at a CTA barrier.
+        std::vector<int> bcol;
+        int nb_col = 0;
+        for (int K = std::max(1, ((int)faces.size() + kColorCap - 1) / kColorCap); K <= 64 && nb_col == 0; K++) {
+            std::vector<uint64_t> u2(ce - cb, 0);
+            std::vector<int> c2(K, 0);
+            bcol.assign(faces.size(), 0);
+            bool fits = true;
+            for (size_t i = 0; i < faces.size() && fits; i++) {
+                const int f = faces[i];
+                const int lL = local[h.face_cells[2 * f]], lR = local[h.face_cells[2 * f + 1]];
+                const uint64_t busy = (lL >= 0 ? u2[lL] : 0) | (lR >= 0 ? u2[lR] : 0);
+                int c = -1;
+                for (int k = 0; k < K; k++)
+                    if (!((busy >> k) & 1ull) && c2[k] < kColorCap && (c < 0 || c2[k] < c2[c])) c = k;
+                if (c < 0) fits = false;
+                else {
+                    bcol[i] = c;
+                    c2[c]++;
+                    if (lL >= 0) u2[lL] |= 1ull << c;
+                    if (lR >= 0) u2[lR] |= 1ull << c;
+                }
+            }
+            if (fits) nb_col = K;
+        }
+        if (nb_col == 0) throw std::invalid_argument("tile face colouring needs more than 64 colours");
+        t.max_colors = std::max(t.max_colors, nb_col);
+        std::vector<int> aorder(faces.size());
+        for (size_t i = 0; i < faces.size(); i++) aorder[i] = (int)i;
+        std::stable_sort(aorder.begin(), aorder.end(), [&](int a, int b) { return bcol[a] < bcol[b]; });
+        for (size_t q = 0; q < aorder.size(); q++) {
+            if (q == 0 || bcol[aorder[q - 1]] != bcol[aorder[q]]) t.col_start.push_back(base + (int)q);
+            t.tf_adj.push_back((uint16_t)pos[aorder[q]]);
         }
         t.col_start.push_back(base + (int)order.size());
         t.col_base.push_back((int)t.col_start.size());
