@@ -713,10 +713,10 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
     const int t = blockIdx.x;
     const int fb = M.tile_face_ptr[t], fe = M.tile_face_ptr[t + 1];
     bool ok = true, rok = true;
-    // FP64 and tangent passes take the faces in global order (neighbouring threads on neighbouring
-    // faces), the mixed pass in record order: each the faster by measurement
+    // faces in global order: neighbouring threads on neighbouring faces (faster than the record order
+    // by measurement)
     for (int k = fb + threadIdx.x; k < fe; k += blockDim.x) {
-        const int i = std::is_same<G, float>::value ? k : fb + M.tf_fwd[k];
+        const int i = fb + M.tf_fwd[k];
         const int2 lr = M.tf_cells[i];
         double normal[DIM], fdx[6];
 #pragma unroll
