@@ -398,7 +398,6 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->col_base.upload(tl.col_base.data(), tl.col_base.size());
         fv->col_start.upload(tl.col_start.data(), tl.col_start.size());
         fv->tf_slot.upload(tl.tf_slot.data(), tl.tf_slot.size());
-        fv->tf_fwd.upload(tl.tf_fwd.data(), tl.tf_fwd.size());
         fv->tf_adj.upload(tl.tf_adj.data(), tl.tf_adj.size());
         fv->tf_nb.upload(tl.tf_nb.data(), tl.tf_nb.size());
         fv->face_nb.upload(tl.face_nb.data(), tl.face_nb.size());
@@ -554,7 +553,6 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.tf_fdx = fv->tf_fdx.p;
         M.tc_fptr = fv->tc_fptr.p;
         M.tc_face = fv->tc_face.p;
-        M.tf_fwd = fv->tf_fwd.p;
         M.tf_adj = fv->tf_adj.p;
         M.col_base = fv->col_base.p;
         M.col_start = fv->col_start.p;

@@ -87,7 +87,7 @@ struct abl_fv {
     // adjoint: tile face colours and slots, non-owned records
     abl::DevBuf<int> col_base, col_start, tf_nb, face_nb, nonowned;
     abl::DevBuf<uint32_t> tf_slot;
-    abl::DevBuf<uint16_t> tf_fwd, tf_adj;
+    abl::DevBuf<uint16_t> tf_adj;
     int tile_max_cells = 0, n_nb = 0;
     // optional per-kernel timing of the last evaluation
     bool profile = false;

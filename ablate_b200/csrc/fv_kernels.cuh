@@ -51,8 +51,7 @@ struct DevMesh {
     const int* col_base;
     const int* col_start;
     const uint32_t* tf_slot;
-    const uint16_t* tf_fwd;  // per tile, the record position of the k-th face in global order
-    const uint16_t* tf_adj;  // per tile, the record position of the k-th face in adjoint colour order
+    const uint16_t* tf_adj;  // per tile, the record of the k-th face in adjoint colour order
     const int* tf_nb;
     const int* face_nb;
     int n_nonowned;
@@ -713,10 +712,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
     const int t = blockIdx.x;
     const int fb = M.tile_face_ptr[t], fe = M.tile_face_ptr[t + 1];
     bool ok = true, rok = true;
-    // faces in global order: neighbouring threads on neighbouring faces (faster than the record order
-    // by measurement)
-    for (int k = fb + threadIdx.x; k < fe; k += blockDim.x) {
-        const int i = fb + M.tf_fwd[k];
+    for (int i = fb + threadIdx.x; i < fe; i += blockDim.x) {
         const int2 lr = M.tf_cells[i];
         double normal[DIM], fdx[6];
 #pragma unroll

@@ -188,10 +188,10 @@ inline void lsq_pinv(int n, int dim, const double* B, double* W) {
 // the face geometry copied into tile order so the kernel streams it, and for every tile cell the
 // (local face, side) pairs in ascending global face order.
 //
-// Within a tile the faces are greedily coloured so that no two faces of one colour touch the same
-// tile cell, and stored colour by colour (ascending face order inside a colour). The adjoint kernel
-// accumulates per-cell sums in shared memory one colour at a time, which needs no atomics and fixes
-// the summation order. A face with a side that is not an owned cell (a boundary ghost or a partition
+// The face records of a tile are in ascending face order. For the adjoint they are also coloured so
+// that no two faces of one colour touch the same tile cell, and listed colour by colour (tf_adj,
+// col_start). The adjoint kernel accumulates per-cell sums in shared memory one colour at a time,
+// which needs no atomics and fixes the summation order. A face with a side that is not an owned cell (a boundary ghost or a partition
 // halo) is in exactly one tile; its contribution to that side goes to a per-face record (nb index).
 struct Tiles {
     int n_tiles = 0;
@@ -205,8 +205,7 @@ struct Tiles {
     std::vector<int32_t> tc_fptr;         // [n_owned+1] per tile cell into tc_face
     std::vector<uint16_t> tc_face;        // local face index | side << 15
     std::vector<uint32_t> tf_slot;        // [ntf] tile-local slot of L | of R << 16 (0xffff: not a tile cell)
-    std::vector<uint16_t> tf_fwd;         // [ntf] per tile, the record position of its k-th face in global order
-    std::vector<uint16_t> tf_adj;         // [ntf] per tile, the record position of its k-th face in adjoint colour order
+    std::vector<uint16_t> tf_adj;         // [ntf] per tile, the record of its k-th face in adjoint colour order
     std::vector<int32_t> tf_nb;           // [ntf] record of the non-owned side, -1 if both sides are owned
     std::vector<int32_t> col_base;        // [n_tiles+1] into col_start
     std::vector<int32_t> col_start;       // per tile: first position (in tf_adj) of each adjoint colour, then the end
@@ -266,8 +265,6 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
     t.face_nb.assign(h.n_faces, -1);
     for (int f : h.flux_faces)
         if (h.kind[h.face_cells[2 * f]] != ABL_CELL_OWNED || h.kind[h.face_cells[2 * f + 1]] != ABL_CELL_OWNED) t.face_nb[f] = t.n_nb++;
-    std::vector<uint64_t> used;
-    std::vector<int> color, order, pos, count;
     for (int k = 0; k < t.n_tiles; k++) {
         const int cb = t.cell_ptr[k], ce = t.cell_ptr[k + 1];
         faces.clear();
@@ -281,35 +278,10 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         if (faces.size() > 0x7fff) throw std::invalid_argument("tile has too many faces");
         t.max_faces = std::max(t.max_faces, (int)faces.size());
         lists.assign(ce - cb, {});
-        // first-fit colouring over the tile cells each face touches, at most kColorCap faces per colour:
-        // it orders the face records
-        used.assign(ce - cb, 0);
-        color.assign(faces.size(), 0);
-        count.assign(64, 0);
-        int ncol = 0;
-        for (size_t i = 0; i < faces.size(); i++) {
-            const int f = faces[i];
-            const int lL = local[h.face_cells[2 * f]], lR = local[h.face_cells[2 * f + 1]];
-            const uint64_t busy = (lL >= 0 ? used[lL] : 0) | (lR >= 0 ? used[lR] : 0);
-            int c = 0;
-            while (c < 64 && (((busy >> c) & 1ull) || count[c] >= kColorCap)) c++;
-            if (c == 64) throw std::invalid_argument("tile face colouring needs more than 64 colours");
-            color[i] = c;
-            count[c]++;
-            ncol = std::max(ncol, c + 1);
-            if (lL >= 0) used[lL] |= 1ull << c;
-            if (lR >= 0) used[lR] |= 1ull << c;
-        }
-        (void)ncol;
-        // records in first-fit colour order (the order the mixed-precision flux pass reads fastest)
-        order.resize(faces.size());
-        for (size_t i = 0; i < faces.size(); i++) order[i] = (int)i;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return color[a] < color[b]; });
-        pos.assign(faces.size(), 0);
+        // face records in global face order (the flux pass reads them in this order, neighbouring
+        // threads on neighbouring faces: the fastest of the orders measured)
         const int base = (int)(t.tf_cells.size() / 2);
-        for (size_t q = 0; q < order.size(); q++) {
-            const int i = order[q];
-            pos[i] = (int)q;
+        for (size_t i = 0; i < faces.size(); i++) {
             const int f = faces[i];
             const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
             t.tf_cells.push_back(L);
@@ -319,7 +291,6 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             t.tf_slot.push_back((uint32_t)(local[L] >= 0 ? local[L] : 0xffff) | ((uint32_t)(local[R] >= 0 ? local[R] : 0xffff) << 16));
             t.tf_nb.push_back(t.face_nb[f]);
         }
-        for (size_t i = 0; i < faces.size(); i++) t.tf_fwd.push_back((uint16_t)pos[i]);
         // the adjoint's colouring: balanced greedy. With K colours allowed each face takes the
         // least-filled colour free at both its cells; K starts at the bound ceil(faces / kColorCap) and
         // grows until every face fits. On an 8x8x4 hex tile (896 faces) that is 8 passes of 112 faces
@@ -355,16 +326,16 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
         std::stable_sort(aorder.begin(), aorder.end(), [&](int a, int b) { return bcol[a] < bcol[b]; });
         for (size_t q = 0; q < aorder.size(); q++) {
             if (q == 0 || bcol[aorder[q - 1]] != bcol[aorder[q]]) t.col_start.push_back(base + (int)q);
-            t.tf_adj.push_back((uint16_t)pos[aorder[q]]);
+            t.tf_adj.push_back((uint16_t)aorder[q]);
         }
-        t.col_start.push_back(base + (int)order.size());
+        t.col_start.push_back(base + (int)faces.size());
         t.col_base.push_back((int)t.col_start.size());
-        // per-cell lists in ascending global face order, pointing at the colour-ordered positions
+        // per-cell lists in ascending global face order, pointing at the face records
         for (size_t i = 0; i < faces.size(); i++) {
             const int f = faces[i];
             const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
-            if (local[L] >= 0) lists[local[L]].push_back((uint16_t)pos[i]);
-            if (local[R] >= 0) lists[local[R]].push_back((uint16_t)(pos[i] | 0x8000));
+            if (local[L] >= 0) lists[local[L]].push_back((uint16_t)i);
+            if (local[R] >= 0) lists[local[R]].push_back((uint16_t)(i | 0x8000));
         }
         for (int j = cb; j < ce; j++) {
             t.tc_fptr[j + 1] = t.tc_fptr[j] + (int)lists[j - cb].size();
