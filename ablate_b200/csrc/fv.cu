@@ -404,10 +404,10 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->n_nb = tl.n_nb;
         for (int k = 0; k < tl.n_tiles; k++) fv->tile_max_cells = std::max(fv->tile_max_cells, tl.cell_ptr[k + 1] - tl.cell_ptr[k]);
         {
-            std::vector<int32_t> no;
-            for (int c = 0; c < h.n_cells; c++)
-                if (h.kind[c] != ABL_CELL_OWNED) no.push_back(c);
+            std::vector<int32_t> no, ow;
+            for (int c = 0; c < h.n_cells; c++) (h.kind[c] != ABL_CELL_OWNED ? no : ow).push_back(c);
             fv->nonowned.upload(no.data(), no.size());
+            fv->owned_rows.upload(ow.data(), ow.size());
         }
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
@@ -1124,6 +1124,38 @@ int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, i
         }
         ABL_DISPATCH(fv, run_normalize, U_dev, s);
         ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+    });
+}
+
+int abl_fv_download_owned(abl_fv* fv, const double* src_dev, int width, double* host, void* stream) {
+    return guarded([&] {
+        if (!fv || !src_dev || !host || width <= 0) throw std::invalid_argument("abl_fv_download_owned: bad argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int64_t n = (int64_t)fv->owned_rows.n;
+        if (n == 0) return;
+        const size_t count = (size_t)n * width;
+        if (fv->io_rows.n < count) fv->io_rows.alloc(count);
+        k_rows<0><<<blocks_for(n * width, 256), 256, 0, s>>>(src_dev, width, fv->owned_rows.p, n, fv->io_rows.p);
+        check_launch();
+        ABL_CUDA(cudaMemcpyAsync(host, fv->io_rows.p, count * sizeof(double), cudaMemcpyDeviceToHost, s));
+        ABL_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int abl_fv_upload_owned(abl_fv* fv, const double* host, int width, double* dst_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !dst_dev || !host || width <= 0) throw std::invalid_argument("abl_fv_upload_owned: bad argument");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const int64_t n = (int64_t)fv->owned_rows.n;
+        if (n == 0) return;
+        const size_t count = (size_t)n * width;
+        if (fv->io_rows.n < count) fv->io_rows.alloc(count);
+        ABL_CUDA(cudaMemcpyAsync(fv->io_rows.p, host, count * sizeof(double), cudaMemcpyHostToDevice, s));
+        k_rows<1><<<blocks_for(n * width, 256), 256, 0, s>>>(fv->io_rows.p, width, fv->owned_rows.p, n, dst_dev);
+        check_launch();
+        ABL_CUDA(cudaStreamSynchronize(s));
     });
 }
 

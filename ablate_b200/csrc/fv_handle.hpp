@@ -115,6 +115,9 @@ struct abl_fv {
     // ghosts grouped by interior neighbour (adjoint of the fill), per-ghost value adjoints
     int n_gseg = 0;
     abl::DevBuf<int> gseg_ptr, gseg_nbr, gseg_ghost;
+    // owned rows in ascending local order (the rank's part of the PETSc global vector) and a staging buffer
+    abl::DevBuf<int> owned_rows;
+    abl::DevBuf<double> io_rows;
     abl::DevBuf<double> ghost_vbar, bc_vbar;
     int n_bc = 1;
     // wall-pressure functional: distinct cells, weights, per-block partial sums

@@ -454,6 +454,22 @@ class FiniteVolumeSolver:
             dt = match(nxt, t)
         return n
 
+    # ---- output and restart: the owned rows (the PETSc global vector of this rank) -----------------
+    def DownloadOwnedDevice(self, src_ptr: int, width: int | None = None, stream: int = 0) -> np.ndarray:
+        """Owned rows of a device array (state by default; width = naux for the aux fields), ascending
+        local cell order."""
+        width = self.nc if width is None else int(width)
+        n = int(np.count_nonzero(np.asarray(self.mesh.cell_kind) == L.CELL_OWNED))
+        out = np.empty((n, width))
+        L.check(L.lib.abl_fv_download_owned(self.handle, C.c_void_p(src_ptr), width, out.ctypes.data_as(C.c_void_p), C.c_void_p(stream)),
+                "abl_fv_download_owned")
+        return out
+
+    def UploadOwnedDevice(self, rows: np.ndarray, dst_ptr: int, stream: int = 0):
+        rows = np.ascontiguousarray(rows, dtype=np.float64)
+        L.check(L.lib.abl_fv_upload_owned(self.handle, rows.ctypes.data_as(C.c_void_p), rows.shape[1], C.c_void_p(dst_ptr), C.c_void_p(stream)),
+                "abl_fv_upload_owned")
+
     def UpdateAux(self, locX: np.ndarray):
         """Recompute the aux fields (T, u, Y) from host state locX (CellSolver::UpdateAuxFields)."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

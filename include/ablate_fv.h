@@ -327,6 +327,17 @@ int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const 
 #define ABL_STEP_SSPRK3 1
 int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, int precision, void* stream);
 
+/* State download and upload for output and restart. The reference saves the TS solution vector (the
+ * rank's owned cells, in local order: the DM's global vector) through PetscViewerHDF5 in its
+ * Hdf5Serializer monitor and reads it back on restart (src/io/hdf5Serializer.cpp:54-160,
+ * src/finiteVolume/finiteVolumeSolver.cpp:398-442). With the state resident on the GPU, download_owned
+ * copies the owned rows of a device array with `width` doubles per cell (the state, nc; the aux
+ * fields, naux) into host[n_owned][width], ascending local cell order, ready for VecView on that
+ * global vector; upload_owned writes such an array back into the owned rows (ghost and halo rows are
+ * the caller's: fill them and exchange halos after a restart). Both wait for `stream`. */
+int abl_fv_download_owned(abl_fv* fv, const double* src_dev, int width, double* host, void* stream);
+int abl_fv_upload_owned(abl_fv* fv, const double* host, int width, double* dst_dev, void* stream);
+
 /* Halo exchange between ranks of a partitioned mesh (the pack and unpack of DMGlobalToLocal's PetscSF
  * broadcast of the state to ghost/overlap cells, src/solver/timeStepper.cpp:343-344). Row i of a
  * width-column FP64 array is copied to or from a contiguous message buffer on `stream`:

@@ -120,3 +120,25 @@ def test_explicit_steps_match_the_oracle(name, scheme):
     # the increments are what the steps compute: compare them relative to their own size
     inc_ref, inc = U[owned] - w.U[owned], got[owned] - w.U[owned]
     assert np.linalg.norm(inc - inc_ref) <= 1e-10 * np.linalg.norm(inc_ref)
+
+
+@pytest.mark.parametrize("name", ["sod2d_ausm_upwind", "species3d_ns5", "tets3d_pg_minmod"])
+def test_owned_rows_download_and_upload(name):
+    """The owned rows leave and re-enter the device unchanged, in ascending local order (the rank's
+    global vector), and an upload touches no other row."""
+    torch = pytest.importorskip("torch")
+    w = R.case(name)
+    s = w.solver()
+    owned = w.mesh.cell_kind == L.CELL_OWNED
+    Ud = _dev(torch, w.U)
+    st = torch.cuda.current_stream().cuda_stream
+    np.testing.assert_array_equal(s.DownloadOwnedDevice(Ud.data_ptr(), stream=st), w.U[owned])
+    rng = np.random.default_rng(9)
+    new = rng.standard_normal((int(owned.sum()), w.U.shape[1]))
+    s.UploadOwnedDevice(new, Ud.data_ptr(), st)
+    got = Ud.cpu().numpy()
+    np.testing.assert_array_equal(got[owned], new)
+    np.testing.assert_array_equal(got[~owned], w.U[~owned])
+    aux = initial_aux(w)
+    Ad = _dev(torch, aux)
+    np.testing.assert_array_equal(s.DownloadOwnedDevice(Ad.data_ptr(), aux.shape[1], st), aux[owned])
