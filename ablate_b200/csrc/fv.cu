@@ -408,6 +408,21 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             for (int c = 0; c < h.n_cells; c++) (h.kind[c] != ABL_CELL_OWNED ? no : ow).push_back(c);
             fv->nonowned.upload(no.data(), no.size());
             fv->owned_rows.upload(ow.data(), ow.size());
+            if (!ow.empty() && ow.back() - ow.front() + 1 == (int)ow.size()) {
+                fv->owned_lo = ow.front();
+                fv->owned_hi = ow.back() + 1;
+            }
+            // output chunks of the host-buffer RHS: possible when every tile's cells are one ascending
+            // range and the tiles follow each other
+            bool ranges = fv->owned_hi >= 0 && tl.n_tiles >= abl_fv::kHostChunks;
+            for (size_t j = 1; ranges && j < tl.cells.size(); j++) ranges = tl.cells[j] == tl.cells[j - 1] + 1;
+            if (ranges) {
+                for (int q = 0; q <= abl_fv::kHostChunks; q++) {
+                    const int tq = (int)((int64_t)tl.n_tiles * q / abl_fv::kHostChunks);
+                    fv->chunk_tile.push_back(tq);
+                    fv->chunk_row.push_back(tq < tl.n_tiles ? tl.cells[tl.cell_ptr[tq]] : fv->owned_hi);
+                }
+            }
         }
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
@@ -582,6 +597,12 @@ int abl_fv_destroy(abl_fv* fv) {
     cudaSetDevice(fv->device);
     for (auto& e : fv->marks)
         if (e) cudaEventDestroy(e);
+    if (fv->host_stream) {
+        cudaStreamDestroy(fv->host_stream);
+        cudaStreamDestroy(fv->copy_stream);
+        cudaEventDestroy(fv->ev_fin);
+        for (auto& e : fv->ev_chunk) cudaEventDestroy(e);
+    }
     delete fv;
     return ABL_OK;
 }
@@ -725,17 +746,44 @@ int abl_fv_update_aux_host(abl_fv* fv, const double* U_host) {
 }
 
 int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision) {
+    struct PipeOff {
+        abl_fv* fv;
+        ~PipeOff() { fv->pipe_active = false; }
+    };
     return guarded([&] {
         if (!fv || !U_host || !F_host) throw std::invalid_argument("abl_fv_rhs_host: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
         const size_t n = (size_t)fv->n_cells * fv->nc;
         if (fv->hU.n != n) fv->hU.alloc(n);
         if (fv->hF.n != n) fv->hF.alloc(n);
-        ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
-        ABL_CUDA(cudaMemcpy(fv->hF.p, F_host, n * sizeof(double), cudaMemcpyHostToDevice));
-        int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision & ~ABL_RHS_OVERWRITE, nullptr);
-        if (rc != ABL_OK) throw AblError(rc, g_last_error);
-        ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (!fv->host_stream) {
+            ABL_CUDA(cudaStreamCreateWithFlags(&fv->host_stream, cudaStreamNonBlocking));
+            ABL_CUDA(cudaStreamCreateWithFlags(&fv->copy_stream, cudaStreamNonBlocking));
+            ABL_CUDA(cudaEventCreateWithFlags(&fv->ev_fin, cudaEventDisableTiming));
+            for (auto& e : fv->ev_chunk) ABL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        // the RHS writes owned rows only: when they are one range, only that range of F travels
+        const bool range = fv->owned_hi >= 0;
+        const size_t f0 = range ? (size_t)fv->owned_lo * fv->nc : 0, f1 = range ? (size_t)fv->owned_hi * fv->nc : n;
+        ABL_CUDA(cudaMemcpyAsync(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice, fv->host_stream));
+        ABL_CUDA(cudaMemcpyAsync(fv->hF.p + f0, F_host + f0, (f1 - f0) * sizeof(double), cudaMemcpyHostToDevice, fv->copy_stream));
+        ABL_CUDA(cudaEventRecord(fv->ev_fin, fv->copy_stream));
+        fv->pipe_active = true;
+        fv->pipe_F_host = F_host;
+        PipeOff off{fv};
+        int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision & ~ABL_RHS_OVERWRITE, fv->host_stream);
+        if (rc != ABL_OK) {
+            cudaStreamSynchronize(fv->host_stream);
+            cudaStreamSynchronize(fv->copy_stream);
+            throw AblError(rc, g_last_error);
+        }
+        if (fv->chunk_tile.empty()) {
+            ABL_CUDA(cudaEventRecord(fv->ev_chunk[0], fv->host_stream));
+            ABL_CUDA(cudaStreamWaitEvent(fv->copy_stream, fv->ev_chunk[0], 0));
+            ABL_CUDA(cudaMemcpyAsync(F_host + f0, fv->hF.p + f0, (f1 - f0) * sizeof(double), cudaMemcpyDeviceToHost, fv->copy_stream));
+        }
+        ABL_CUDA(cudaStreamSynchronize(fv->host_stream));
+        ABL_CUDA(cudaStreamSynchronize(fv->copy_stream));
     });
 }
 

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "fv_adjoint.cuh"
 
@@ -126,6 +127,16 @@ struct abl_fv {
     abl::DevBuf<double> fn_w, fn_partial;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
+    // host-buffer RHS pipeline: F comes in on a copy stream while the gradient pass runs, and goes out
+    // chunk by chunk as the tile pass finishes contiguous row ranges (when the tiles' cells are ranges)
+    static constexpr int kHostChunks = 4;
+    cudaStream_t host_stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t ev_fin = nullptr, ev_chunk[kHostChunks] = {};
+    int owned_lo = 0, owned_hi = -1;   // owned rows are [owned_lo, owned_hi) when contiguous, else owned_hi = -1
+    std::vector<int> chunk_tile;       // tile boundaries of the output chunks (empty: one copy after the pass)
+    std::vector<int> chunk_row;        // their row boundaries
+    bool pipe_active = false;          // set for the duration of one abl_fv_rhs_host call
+    double* pipe_F_host = nullptr;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;
 };
 

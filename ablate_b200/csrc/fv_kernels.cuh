@@ -704,12 +704,12 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
                                                                      const double* __restrict__ dU, const double* __restrict__ aux,
                                                                      const G* __restrict__ grad, const G* __restrict__ agrad,
                                                                      double* __restrict__ F, double* __restrict__ dF, int overwrite,
-                                                                     int* status) {
+                                                                     int* status, int t0 = 0) {
     using D = Dims<DIM, NS>;
     using S = StateOf<G>;
     extern __shared__ double sflux_raw[];
     S* sflux = reinterpret_cast<S*>(sflux_raw);  // [faces of this tile][NC]
-    const int t = blockIdx.x;
+    const int t = t0 + blockIdx.x;
     const int fb = M.tile_face_ptr[t], fe = M.tile_face_ptr[t + 1];
     bool ok = true, rok = true;
     for (int i = fb + threadIdx.x; i < fe; i += blockDim.x) {

@@ -12,8 +12,32 @@ void launch_tile(abl_fv* fv, const double* U, const double* dU, const G* grad, c
     const int smem = fv->tile_smem * (std::is_same<G, Dual>::value ? 2 : 1);
     if (smem > 227 * 1024) throw AblError(ABL_ERR_UNSUPPORTED, "tile flux buffer exceeds shared memory for this species count");
     ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    kern<<<fv->mesh.n_tiles, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p);
-    check_launch();
+    if (!fv->pipe_active) {
+        kern<<<fv->mesh.n_tiles, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p, 0);
+        check_launch();
+        return;
+    }
+    // host-buffer call: the residual rows must have arrived; each chunk of tiles, once done, sends its
+    // rows back on the copy stream while the next chunk runs
+    ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_fin, 0));
+    const int nch = fv->chunk_tile.empty() ? 0 : (int)fv->chunk_tile.size() - 1;
+    if (nch == 0) {
+        kern<<<fv->mesh.n_tiles, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p, 0);
+        check_launch();
+        return;
+    }
+    for (int q = 0; q < nch; q++) {
+        const int ta = fv->chunk_tile[q], tb = fv->chunk_tile[q + 1];
+        if (tb > ta) {
+            kern<<<tb - ta, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p, ta);
+            check_launch();
+        }
+        ABL_CUDA(cudaEventRecord(fv->ev_chunk[q], s));
+        ABL_CUDA(cudaStreamWaitEvent(fv->copy_stream, fv->ev_chunk[q], 0));
+        const size_t r0 = (size_t)fv->chunk_row[q] * fv->nc, r1 = (size_t)fv->chunk_row[q + 1] * fv->nc;
+        if (r1 > r0)
+            ABL_CUDA(cudaMemcpyAsync(fv->pipe_F_host + r0, F + r0, (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost, fv->copy_stream));
+    }
 }
 
 // shared memory for the neighbour differences the limiter reuses (none when it would not fit)
