@@ -600,7 +600,9 @@ int abl_fv_destroy(abl_fv* fv) {
     if (fv->host_stream) {
         cudaStreamDestroy(fv->host_stream);
         cudaStreamDestroy(fv->copy_stream);
-        cudaEventDestroy(fv->ev_fin);
+        cudaStreamDestroy(fv->out_stream);
+        cudaEventDestroy(fv->ev_u);
+        for (auto& e : fv->ev_in) cudaEventDestroy(e);
         for (auto& e : fv->ev_chunk) cudaEventDestroy(e);
     }
     delete fv;
@@ -759,15 +761,29 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
         if (!fv->host_stream) {
             ABL_CUDA(cudaStreamCreateWithFlags(&fv->host_stream, cudaStreamNonBlocking));
             ABL_CUDA(cudaStreamCreateWithFlags(&fv->copy_stream, cudaStreamNonBlocking));
-            ABL_CUDA(cudaEventCreateWithFlags(&fv->ev_fin, cudaEventDisableTiming));
+            ABL_CUDA(cudaStreamCreateWithFlags(&fv->out_stream, cudaStreamNonBlocking));
+            ABL_CUDA(cudaEventCreateWithFlags(&fv->ev_u, cudaEventDisableTiming));
+            for (auto& e : fv->ev_in) ABL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             for (auto& e : fv->ev_chunk) ABL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
         // the RHS writes owned rows only: when they are one range, only that range of F travels
         const bool range = fv->owned_hi >= 0;
         const size_t f0 = range ? (size_t)fv->owned_lo * fv->nc : 0, f1 = range ? (size_t)fv->owned_hi * fv->nc : n;
         ABL_CUDA(cudaMemcpyAsync(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice, fv->host_stream));
-        ABL_CUDA(cudaMemcpyAsync(fv->hF.p + f0, F_host + f0, (f1 - f0) * sizeof(double), cudaMemcpyHostToDevice, fv->copy_stream));
-        ABL_CUDA(cudaEventRecord(fv->ev_fin, fv->copy_stream));
+        ABL_CUDA(cudaEventRecord(fv->ev_u, fv->host_stream));
+        // the residual's rows follow the state in the same copy direction, chunk by chunk
+        ABL_CUDA(cudaStreamWaitEvent(fv->copy_stream, fv->ev_u, 0));
+        if (fv->chunk_tile.empty()) {
+            ABL_CUDA(cudaMemcpyAsync(fv->hF.p + f0, F_host + f0, (f1 - f0) * sizeof(double), cudaMemcpyHostToDevice, fv->copy_stream));
+            ABL_CUDA(cudaEventRecord(fv->ev_in[0], fv->copy_stream));
+        } else {
+            for (size_t q = 0; q + 1 < fv->chunk_row.size(); q++) {
+                const size_t r0 = (size_t)fv->chunk_row[q] * fv->nc, r1 = (size_t)fv->chunk_row[q + 1] * fv->nc;
+                if (r1 > r0)
+                    ABL_CUDA(cudaMemcpyAsync(fv->hF.p + r0, F_host + r0, (r1 - r0) * sizeof(double), cudaMemcpyHostToDevice, fv->copy_stream));
+                ABL_CUDA(cudaEventRecord(fv->ev_in[q], fv->copy_stream));
+            }
+        }
         fv->pipe_active = true;
         fv->pipe_F_host = F_host;
         PipeOff off{fv};
@@ -775,15 +791,17 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
         if (rc != ABL_OK) {
             cudaStreamSynchronize(fv->host_stream);
             cudaStreamSynchronize(fv->copy_stream);
+            cudaStreamSynchronize(fv->out_stream);
             throw AblError(rc, g_last_error);
         }
         if (fv->chunk_tile.empty()) {
             ABL_CUDA(cudaEventRecord(fv->ev_chunk[0], fv->host_stream));
-            ABL_CUDA(cudaStreamWaitEvent(fv->copy_stream, fv->ev_chunk[0], 0));
-            ABL_CUDA(cudaMemcpyAsync(F_host + f0, fv->hF.p + f0, (f1 - f0) * sizeof(double), cudaMemcpyDeviceToHost, fv->copy_stream));
+            ABL_CUDA(cudaStreamWaitEvent(fv->out_stream, fv->ev_chunk[0], 0));
+            ABL_CUDA(cudaMemcpyAsync(F_host + f0, fv->hF.p + f0, (f1 - f0) * sizeof(double), cudaMemcpyDeviceToHost, fv->out_stream));
         }
         ABL_CUDA(cudaStreamSynchronize(fv->host_stream));
         ABL_CUDA(cudaStreamSynchronize(fv->copy_stream));
+        ABL_CUDA(cudaStreamSynchronize(fv->out_stream));
     });
 }
 

@@ -127,11 +127,12 @@ struct abl_fv {
     abl::DevBuf<double> fn_w, fn_partial;
     // host-pointer paths
     abl::DevBuf<double> hU, hF, hdU, hdF;
-    // host-buffer RHS pipeline: F comes in on a copy stream while the gradient pass runs, and goes out
-    // chunk by chunk as the tile pass finishes contiguous row ranges (when the tiles' cells are ranges)
+    // host-buffer RHS pipeline: after the state, F comes in on a copy stream while the gradient pass
+    // runs, chunk by chunk, each tile chunk waiting for its own rows; finished chunks go out on a third
+    // stream (the other copy direction) while the next ones run (when the tiles' cells are row ranges)
     static constexpr int kHostChunks = 4;
-    cudaStream_t host_stream = nullptr, copy_stream = nullptr;
-    cudaEvent_t ev_fin = nullptr, ev_chunk[kHostChunks] = {};
+    cudaStream_t host_stream = nullptr, copy_stream = nullptr, out_stream = nullptr;
+    cudaEvent_t ev_u = nullptr, ev_in[kHostChunks] = {}, ev_chunk[kHostChunks] = {};
     int owned_lo = 0, owned_hi = -1;   // owned rows are [owned_lo, owned_hi) when contiguous, else owned_hi = -1
     std::vector<int> chunk_tile;       // tile boundaries of the output chunks (empty: one copy after the pass)
     std::vector<int> chunk_row;        // their row boundaries

@@ -17,26 +17,27 @@ void launch_tile(abl_fv* fv, const double* U, const double* dU, const G* grad, c
         check_launch();
         return;
     }
-    // host-buffer call: the residual rows must have arrived; each chunk of tiles, once done, sends its
-    // rows back on the copy stream while the next chunk runs
-    ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_fin, 0));
+    // host-buffer call: each chunk of tiles waits for its residual rows, and once done sends them back on
+    // the output stream while the next chunk runs
     const int nch = fv->chunk_tile.empty() ? 0 : (int)fv->chunk_tile.size() - 1;
     if (nch == 0) {
+        ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_in[0], 0));
         kern<<<fv->mesh.n_tiles, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p, 0);
         check_launch();
         return;
     }
     for (int q = 0; q < nch; q++) {
         const int ta = fv->chunk_tile[q], tb = fv->chunk_tile[q + 1];
+        ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_in[q], 0));
         if (tb > ta) {
             kern<<<tb - ta, 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, F, dF, overwrite, fv->status.p, ta);
             check_launch();
         }
         ABL_CUDA(cudaEventRecord(fv->ev_chunk[q], s));
-        ABL_CUDA(cudaStreamWaitEvent(fv->copy_stream, fv->ev_chunk[q], 0));
+        ABL_CUDA(cudaStreamWaitEvent(fv->out_stream, fv->ev_chunk[q], 0));
         const size_t r0 = (size_t)fv->chunk_row[q] * fv->nc, r1 = (size_t)fv->chunk_row[q + 1] * fv->nc;
         if (r1 > r0)
-            ABL_CUDA(cudaMemcpyAsync(fv->pipe_F_host + r0, F + r0, (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost, fv->copy_stream));
+            ABL_CUDA(cudaMemcpyAsync(fv->pipe_F_host + r0, F + r0, (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost, fv->out_stream));
     }
 }
 
