@@ -130,7 +130,7 @@ struct abl_fv {
     // host-buffer RHS pipeline: after the state, F comes in on a copy stream while the gradient pass
     // runs, chunk by chunk, each tile chunk waiting for its own rows; finished chunks go out on a third
     // stream (the other copy direction) while the next ones run (when the tiles' cells are row ranges)
-    static constexpr int kHostChunks = 4;
+    static constexpr int kHostChunks = 16;
     cudaStream_t host_stream = nullptr, copy_stream = nullptr, out_stream = nullptr;
     cudaEvent_t ev_u = nullptr, ev_in[kHostChunks] = {}, ev_chunk[kHostChunks] = {};
     int owned_lo = 0, owned_hi = -1;   // owned rows are [owned_lo, owned_hi) when contiguous, else owned_hi = -1
