@@ -100,6 +100,7 @@ SIGNATURES = {
     "abl_fv_fill_ghosts_jvp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_set_jvp_mode": (C.c_int, [C.c_void_p, C.c_int]),
     "abl_fv_download_owned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "abl_fv_step_cfl": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "abl_fv_upload_owned": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "abl_fv_fill_ghosts_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_set_pressure_functional": (C.c_int, [C.c_void_p, C.c_int32, _ip, C.c_void_p]),

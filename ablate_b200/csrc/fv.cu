@@ -1032,8 +1032,8 @@ void run_pressure_functional(abl_fv* fv, const double* U, double* Ub, cudaStream
 }
 template <int DIM, int NS>
 void run_cfl_dt(abl_fv* fv, const double* U, double cfl, cudaStream_t s) {
-    const double big = DBL_MAX;
-    ABL_CUDA(cudaMemcpyAsync(fv->dt_bits.p, &big, sizeof(double), cudaMemcpyHostToDevice, s));
+    // all bits set: above every positive double's bit pattern, the identity of the unsigned minimum
+    ABL_CUDA(cudaMemsetAsync(fv->dt_bits.p, 0xff, sizeof(unsigned long long), s));
     k_cfl_dt<DIM, NS><<<blocks_for(fv->n_cells, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->rmin.p, cfl, fv->dt_bits.p, fv->status.p);
     check_launch();
 }
@@ -1045,6 +1045,12 @@ void run_normalize(abl_fv* fv, double* U, cudaStream_t s) {
 }
 void rk_stage(abl_fv* fv, double a, const double* U0, double b, const double* Us, double dt, const double* F, double* Uout, cudaStream_t s) {
     k_rk_stage<><<<blocks_for((int64_t)fv->n_cells * fv->nc, 256), 256, 0, s>>>(fv->kind.p, fv->nc, fv->n_cells, a, U0, b, Us, dt, F, Uout);
+    check_launch();
+}
+// the same stage with the step taken from the CFL reduction's result on the device
+void rk_stage_dev(abl_fv* fv, double a, const double* U0, double b, const double* Us, const double* F, double* Uout, double* time, cudaStream_t s) {
+    k_rk_stage_dev<><<<blocks_for((int64_t)fv->n_cells * fv->nc, 256), 256, 0, s>>>(fv->kind.p, fv->nc, fv->n_cells, a, U0, b, Us, fv->dt_bits.p, F,
+                                                                                   Uout, time);
     check_launch();
 }
 }  // namespace
@@ -1222,6 +1228,40 @@ int abl_fv_upload_owned(abl_fv* fv, const double* host, int width, double* dst_d
         k_rows<1><<<blocks_for(n * width, 256), 256, 0, s>>>(fv->io_rows.p, width, fv->owned_rows.p, n, dst_dev);
         check_launch();
         ABL_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int abl_fv_step_cfl(abl_fv* fv, int scheme, double cfl, double* U_dev, int precision, double* time_dev, void* stream) {
+    return guarded([&] {
+        if (!fv || !U_dev) throw std::invalid_argument("abl_fv_step_cfl: NULL argument");
+        if (!(cfl > 0)) throw std::invalid_argument("abl_fv_step_cfl: cfl must be positive");
+        if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
+        if (scheme != ABL_STEP_EULER && scheme != ABL_STEP_SSPRK3) throw std::invalid_argument("abl_fv_step_cfl: unknown scheme");
+        ABL_CUDA(cudaSetDevice(fv->device));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t n = (size_t)fv->n_cells * fv->nc;
+        if (fv->step_F.n != n) fv->step_F.alloc(n);
+        double* F = fv->step_F.p;
+        // the CFL step of the state the step starts from, as abl_fv_cfl_dt computes it (ghosts filled first)
+        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+        ABL_DISPATCH(fv, run_cfl_dt, U_dev, cfl, s);
+        dispatch_rhs(fv, U_dev, F, precision, 1, s);
+        if (scheme == ABL_STEP_EULER) {
+            rk_stage_dev(fv, 0.0, nullptr, 1.0, U_dev, F, U_dev, time_dev, s);
+        } else {
+            if (fv->step_U1.n != n) fv->step_U1.alloc(n);
+            double* U1 = fv->step_U1.p;
+            ABL_CUDA(cudaMemcpyAsync(U1, U_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            rk_stage_dev(fv, 0.0, nullptr, 1.0, U_dev, F, U1, nullptr, s);
+            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            dispatch_rhs(fv, U1, F, precision, 1, s);
+            rk_stage_dev(fv, 0.75, U_dev, 0.25, U1, F, U1, nullptr, s);
+            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            dispatch_rhs(fv, U1, F, precision, 1, s);
+            rk_stage_dev(fv, 1.0 / 3.0, U_dev, 2.0 / 3.0, U1, F, U_dev, time_dev, s);
+        }
+        ABL_DISPATCH(fv, run_normalize, U_dev, s);
+        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
     });
 }
 

@@ -142,6 +142,21 @@ __global__ void __launch_bounds__(256) k_rk_stage(const uint8_t* __restrict__ ki
     Uout[e] = a == 0.0 ? b * s : a * U0[e] + b * s;
 }
 
+// k_rk_stage with the step read from the device: dt = the double whose bits the CFL reduction left in
+// *dt_bits. Thread 0 of block 0 adds dt to *time when `time` is not null.
+template <int UNUSED = 0>
+__global__ void __launch_bounds__(256) k_rk_stage_dev(const uint8_t* __restrict__ kind, int nc, int n_cells, double a, const double* U0, double b,
+                                                      const double* Us, const unsigned long long* __restrict__ dt_bits, const double* __restrict__ F,
+                                                      double* Uout, double* time) {
+    const double dt = __longlong_as_double((long long)*dt_bits);
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (time && e == 0) *time += dt;
+    if (e >= (int64_t)n_cells * nc) return;
+    if (kind[e / nc] != ABL_CELL_OWNED) return;
+    const double s = Us[e] + dt * F[e];
+    Uout[e] = a == 0.0 ? b * s : a * U0[e] + b * s;
+}
+
 // Ghosts grouped by their interior neighbour: segment s owns ghosts seg_ghost[seg_ptr[s] .. seg_ptr[s+1])
 // (ascending), all next to cell seg_nbr[s]. One thread per segment keeps the sums in a fixed order.
 struct GhostSegments {

@@ -426,6 +426,12 @@ class FiniteVolumeSolver:
     def StepDevice(self, scheme: int, time: float, dt: float, U_ptr: int, precision: int = L.PRECISION_FP64, stream: int = 0):
         L.check(L.lib.abl_fv_step(self.handle, scheme, time, dt, C.c_void_p(U_ptr), precision, C.c_void_p(stream)), "abl_fv_step")
 
+    def StepCflDevice(self, scheme: int, cfl: float, U_ptr: int, precision: int = L.PRECISION_FP64, time_ptr: int = 0, stream: int = 0):
+        """One step with dt = the CFL step of the current state, computed and used on the device (no
+        host synchronisation); dt is added to the device double at time_ptr when given."""
+        L.check(L.lib.abl_fv_step_cfl(self.handle, scheme, float(cfl), C.c_void_p(U_ptr), precision, C.c_void_p(time_ptr or None),
+                                      C.c_void_p(stream)), "abl_fv_step_cfl")
+
     def IntegrateDevice(self, U_ptr: int, t_end: float, cfl: float, scheme: int = L.STEP_EULER, precision: int = L.PRECISION_FP64,
                         dt0: float = 0.1, stream: int = 0) -> int:
         """March the device state to t_end as the reference's TimeStepper does with ts_adapt_type physics:

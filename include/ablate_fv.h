@@ -327,6 +327,12 @@ int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const 
 #define ABL_STEP_SSPRK3 1
 int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, int precision, void* stream);
 
+/* The same step with dt = the CFL step of U_dev's state (abl_fv_cfl_dt, this rank's minimum) computed
+ * and used on the device: nothing returns to the host, so consecutive steps queue back to back on
+ * `stream` (and can be captured in a CUDA graph). When time_dev is not NULL, dt is added to *time_dev
+ * (a device double). Single domain: a partitioned run needs the minimum over ranks first. */
+int abl_fv_step_cfl(abl_fv* fv, int scheme, double cfl, double* U_dev, int precision, double* time_dev, void* stream);
+
 /* State download and upload for output and restart. The reference saves the TS solution vector (the
  * rank's owned cells, in local order: the DM's global vector) through PetscViewerHDF5 in its
  * Hdf5Serializer monitor and reads it back on restart (src/io/hdf5Serializer.cpp:54-160,
