@@ -179,7 +179,11 @@ int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells,
  * src/finiteVolume/finiteVolumeSolver.cpp:233-291). */
 int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int precision, void* stream);
 
-/* Same with host pointers (the plain PETSc Vec case): copies U in, runs abl_fv_rhs, adds into F. */
+/* Same with host pointers (the plain PETSc Vec case): copies U in, runs abl_fv_rhs, adds into F. The
+ * copies run on the handle's own streams, overlapped with the kernels (F's rows in chunks, each sent
+ * back as soon as its tiles are done); the call returns when F_host holds the result. Only the owned
+ * rows of F travel when they are one contiguous range. Pinned host memory makes the copies asynchronous.
+ * A handle serves one call at a time (no two threads on one handle). */
 int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision);
 
 /* Forward tangent (JVP) of abl_fv_rhs at FP64: dF += J(U) dU for owned cells, and F += RHS(U) when F
