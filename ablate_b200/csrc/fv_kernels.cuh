@@ -100,12 +100,13 @@ struct GradRows {
 };
 
 // minimum resident CTAs per SM for __launch_bounds__ (register budget per thread = 65536 / (128 * n)),
-// chosen by timing on the 128^3 case: gradient FP64 4 / FP32 6, tile FP64 4 (no spills at 128
-// registers) / FP32 5; the value+tangent pairs of the tangent kernels 1
+// chosen by timing: on the 128^3 gas gradient FP64 4 / FP32 6, tile FP64 4 (no spills at 128
+// registers) / FP32 5; with 3-5 species 3 (5 species: 2.7 % faster than 2), with more species 2 (9
+// species on tetrahedra: 3 is 14 % slower); the value+tangent pairs of the tangent kernels 1
 template <int NS, class G>
 struct MinBlocks {
-    static constexpr int grad = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : (NS > 0 ? 3 : (sizeof(G) == 8 ? 4 : 6)));
-    static constexpr int tile = std::is_same<G, Dual>::value ? 1 : (NS > 2 ? 2 : (sizeof(G) == 8 ? 4 : 5));
+    static constexpr int grad = std::is_same<G, Dual>::value ? 1 : (NS > 5 ? 2 : (NS > 0 ? 3 : (sizeof(G) == 8 ? 4 : 6)));
+    static constexpr int tile = std::is_same<G, Dual>::value ? 1 : (NS > 5 ? 2 : (NS > 2 ? 3 : (sizeof(G) == 8 ? 4 : 5)));
 };
 
 constexpr int kConeSide = int(1u << 31);
