@@ -285,8 +285,9 @@ unsigned char* noalloc_scratch(int device) {
 }
 
 // =================================================================================================
-// halo pack (SCATTER = 0: dst[i] = src[idx[i]]) and unpack (SCATTER = 1: dst[idx[i]] = src[i]), one
-// thread per element so consecutive threads move consecutive doubles of a row
+// halo pack (SCATTER = 0: dst[i] = src[idx[i]]), unpack (SCATTER = 1: dst[idx[i]] = src[i]) and the
+// adjoint's accumulate (SCATTER = 2: dst[idx[i]] += src[i], indices distinct), one thread per element
+// so consecutive threads move consecutive doubles of a row
 template <int SCATTER>
 __global__ void __launch_bounds__(256) k_rows(const double* __restrict__ src, int width, const int32_t* __restrict__ idx, int64_t n,
                                               double* __restrict__ dst) {
@@ -295,7 +296,9 @@ __global__ void __launch_bounds__(256) k_rows(const double* __restrict__ src, in
     const int64_t i = e / width;
     const int k = (int)(e - i * width);
     const int64_t r = __ldg(idx + i);
-    if (SCATTER)
+    if (SCATTER == 2)
+        dst[r * width + k] += src[i * width + k];
+    else if (SCATTER == 1)
         dst[r * width + k] = src[i * width + k];
     else
         dst[i * width + k] = src[r * width + k];
@@ -1271,6 +1274,16 @@ int abl_rows_gather(const double* src_dev, int width, const int32_t* idx_dev, in
         if (n == 0) return;
         if (!src_dev || !idx_dev || !dst_dev) throw std::invalid_argument("abl_rows_gather: NULL argument");
         k_rows<0><<<blocks_for(n * width, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(src_dev, width, idx_dev, n, dst_dev);
+        check_launch();
+    });
+}
+
+int abl_rows_scatter_add(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream) {
+    return guarded([&] {
+        if (n < 0 || width <= 0) throw std::invalid_argument("abl_rows_scatter_add: bad size");
+        if (n == 0) return;
+        if (!src_dev || !idx_dev || !dst_dev) throw std::invalid_argument("abl_rows_scatter_add: NULL argument");
+        k_rows<2><<<blocks_for(n * width, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(src_dev, width, idx_dev, n, dst_dev);
         check_launch();
     });
 }

@@ -226,6 +226,38 @@ class HaloExchange:
                                                n, C.c_void_p(U.data_ptr()), C.c_void_p(stream)), "abl_rows_scatter")
 
 
+    def exchange_adjoint(self, Ubar):
+        """Transpose of exchange(): the adjoint held in this rank's halo rows goes back to their owners,
+        which add it into the owned rows (peers in ascending order, a fixed summation order); the halo
+        rows are cleared."""
+        torch = self.torch
+        import torch.distributed as dist
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        for p in self.peers:
+            n = self.recv_idx[p].numel()
+            if n:
+                L.check(L.lib.abl_rows_gather(C.c_void_p(Ubar.data_ptr()), self.width, C.c_void_p(self.recv_idx[p].data_ptr()), n,
+                                              C.c_void_p(self.recv_buf[p].data_ptr()), C.c_void_p(stream)), "abl_rows_gather")
+        ops = []
+        for p in self.peers:
+            if self.send_idx[p].numel():
+                ops.append(dist.P2POp(dist.irecv, self.send_buf[p], p, group=self.group))
+            if self.recv_idx[p].numel():
+                ops.append(dist.P2POp(dist.isend, self.recv_buf[p], p, group=self.group))
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+        for p in self.peers:
+            n = self.send_idx[p].numel()
+            if n:
+                L.check(L.lib.abl_rows_scatter_add(C.c_void_p(self.send_buf[p].data_ptr()), self.width,
+                                                   C.c_void_p(self.send_idx[p].data_ptr()), n, C.c_void_p(Ubar.data_ptr()),
+                                                   C.c_void_p(stream)), "abl_rows_scatter_add")
+        for p in self.peers:
+            if self.recv_idx[p].numel():
+                Ubar.index_fill_(0, self.recv_idx[p].long(), 0.0)
+
+
 class DistributedRHS:
     """One rank's RHS of a partitioned mesh: the halo exchange, then the local RHS on the same stream
     (the order TimeStepper::SolverComputeRHSFunction runs DMGlobalToLocal and the RHS in)."""
@@ -248,6 +280,22 @@ class DistributedRHS:
         self.halo.exchange(U)
         stream = self.torch.cuda.current_stream(self.device).cuda_stream
         self.solver.ComputeRHSDevice(time, U.data_ptr(), F.data_ptr(), precision, stream)
+
+    def ComputeJVPDevice(self, time: float, U, dU, dF, F=None):
+        """dF += J(U) dU on the owned rows (and F += RHS(U) when F is given), after refreshing the halo
+        rows of both U and dU."""
+        self.halo.exchange(U)
+        self.halo.exchange(dU)
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        self.solver.ComputeJVPDevice(time, U.data_ptr(), dU.data_ptr(), dF.data_ptr(), F.data_ptr() if F is not None else 0, stream)
+
+    def ComputeVJPDevice(self, time: float, U, Fbar, Ubar):
+        """Ubar += J(U)^T Fbar for the owned rows of the whole partitioned problem: the local adjoint, then
+        the halo rows' share sent back to their owners (exchange_adjoint; Ubar's halo rows are consumed)."""
+        self.halo.exchange(U)
+        stream = self.torch.cuda.current_stream(self.device).cuda_stream
+        self.solver.ComputeVJPDevice(time, U.data_ptr(), Fbar.data_ptr(), Ubar.data_ptr(), stream)
+        self.halo.exchange_adjoint(Ubar)
 
     def close(self):
         self.solver.close()

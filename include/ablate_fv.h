@@ -357,6 +357,12 @@ int abl_fv_upload_owned(abl_fv* fv, const double* host, int width, double* dst_d
 int abl_rows_gather(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream);
 int abl_rows_scatter(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream);
 
+/* The adjoint of the exchange: dst[idx[i]][:] += src[i][:] (the indices of one call distinct). A rank
+ * sends the adjoint of its halo rows back to their owners, which add them into the owned rows, one
+ * peer after another in a fixed order (the transpose of DMGlobalToLocal, a LocalToGlobal with
+ * ADD_VALUES: src/solver/timeStepper.cpp:379-380). */
+int abl_rows_scatter_add(const double* src_dev, int width, const int32_t* idx_dev, int64_t n, double* dst_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
