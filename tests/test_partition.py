@@ -171,3 +171,52 @@ def test_two_gloo_ranks_exchange_halos_and_match_the_single_domain(name):
             p.kill()
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     assert q.get(timeout=5) is True
+
+
+def _exchange_adjoint_numpy(domains, plans, Ub_local):
+    """Transpose of _exchange_numpy: each halo row's adjoint is added into its owner's row (peers in
+    ascending order) and cleared, as HaloExchange.exchange_adjoint does with NCCL."""
+    msgs = {}
+    for d, pl in zip(domains, plans):
+        for p, rows in pl.recv.items():
+            msgs[(d.rank, p)] = Ub_local[d.rank][rows].copy()
+    for d, pl in zip(domains, plans):
+        for p in sorted(pl.send):
+            Ub_local[d.rank][pl.send[p]] += msgs[(p, d.rank)]
+    for d, pl in zip(domains, plans):
+        for p, rows in pl.recv.items():
+            Ub_local[d.rank][rows] = 0.0
+
+
+@pytest.mark.parametrize("name", ["tgv3d_ausmpup_lsq_minmod_visc", "tets3d_pg_minmod"])
+def test_transposed_exchange_is_the_adjoint_of_the_exchange(name):
+    """<E x, y> = <x, E^T y>: E fills every local row from the owned rows of x (the halo exchange), E^T
+    adds the halo rows of y into their owners; x lives on the owned rows, y on all local rows."""
+    w = R.case(name)
+    part = D.partition_cells(w.mesh, 3)
+    domains = [D.submesh(w.mesh, part, r) for r in range(3)]
+    plans = D.all_plans(domains)
+    rng = np.random.default_rng(6)
+    nc = w.U.shape[1]
+    xg = rng.standard_normal((w.mesh.n_cells, nc))
+    X = []
+    for d in domains:
+        a = np.zeros((d.mesh.n_cells, nc))
+        mine = d.owner == d.rank
+        a[mine] = xg[d.gid[mine]]
+        X.append(a)
+    _exchange_numpy(domains, plans, X)
+    Y = [rng.standard_normal((d.mesh.n_cells, nc)) for d in domains]
+    # only the rows the exchange fills carry the pairing: owned rows and exchanged halo rows
+    lhs = 0.0
+    for d, pl, x, y in zip(domains, plans, X, Y):
+        mine = d.owner == d.rank
+        rows = np.concatenate([np.nonzero(mine)[0]] + [r for r in pl.recv.values()])
+        lhs += float(np.sum(x[rows] * y[rows]))
+    Yt = [y.copy() for y in Y]
+    _exchange_adjoint_numpy(domains, plans, Yt)
+    rhs = 0.0
+    for d, x, yt in zip(domains, X, Yt):
+        mine = d.owner == d.rank
+        rhs += float(np.sum(x[mine] * yt[mine]))
+    assert abs(lhs - rhs) <= 1e-12 * sum(float(np.abs(y).sum()) for y in Y)
