@@ -452,16 +452,21 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                     }
                 }
             }
-            fv->cw.upload(cw.data(), cw.size());
-            fv->caw.upload(caw.data(), caw.size());
+            std::vector<double> cwa(6 * ncone);
+            for (size_t i = 0; i < ncone; i++)
+                for (int d = 0; d < 3; d++) {
+                    cwa[6 * i + d] = cw[3 * i + d];
+                    cwa[6 * i + 3 + d] = caw[3 * i + d];
+                }
+            fv->cwa.upload(cwa.data(), cwa.size());
             fv->cv.upload(cv.data(), cv.size());
             fv->cwr.upload(cwr.data(), cwr.size());
             fv->cawr.upload(cawr.data(), cawr.size());
             if (fv->ns == 0) {  // the mixed path's copies (with species it runs the FP64 kernels)
-                std::vector<float> f32(cw.begin(), cw.end());
-                fv->cw32.upload(f32.data(), f32.size());
-                f32.assign(caw.begin(), caw.end());
-                fv->caw32.upload(f32.data(), f32.size());
+                std::vector<float> f32(8 * ncone, 0.0f);
+                for (size_t i = 0; i < ncone; i++)
+                    for (int d = 0; d < 6; d++) f32[8 * i + d] = (float)cwa[6 * i + d];
+                fv->cwa32.upload(f32.data(), f32.size());
                 f32.assign(cv.begin(), cv.end());
                 fv->cv32.upload(f32.data(), f32.size());
                 f32.assign(tl.tf_fdx.begin(), tl.tf_fdx.end());
@@ -580,13 +585,11 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.n_nonowned = (int)fv->nonowned.n;
         M.nonowned = fv->nonowned.p;
         M.wsum = fv->wsum.p;
-        M.cw = fv->cw.p;
-        M.caw = fv->caw.p;
+        M.cwa = fv->cwa.p;
         M.cv = fv->cv.p;
         M.cwr = fv->cwr.p;
         M.cawr = fv->cawr.p;
-        M.cw32 = fv->cw32.p;
-        M.caw32 = fv->caw32.p;
+        M.cwa32 = fv->cwa32.p;
         M.cv32 = fv->cv32.p;
         M.tf_fdx32 = fv->tf_fdx32.p;
         M.max_cone = fv->max_cone;

@@ -57,10 +57,10 @@ struct DevMesh {
     int n_nonowned;
     const int* nonowned;  // cells that are not owned (boundary ghosts, halos)
     const double* wsum;   // [nc][2][3] per cell: sum of its LSQ state weights (non-boundary faces), of its aux weights
-    // per cone entry (cell-major, contiguous per cell): LSQ state weight (0 across a boundary face),
-    // aux (face-interpolant) weight, and the neighbour offset x_n - x_c
-    const double* cw;
-    const double* caw;
+    // per cone entry (cell-major, contiguous per cell): the LSQ state weight (0 across a boundary face)
+    // and the aux (face-interpolant) weight packed in one 48-byte record [w0 w1 w2 a0 a1 a2], and the
+    // neighbour offset x_n - x_c
+    const double* cwa;
     const double* cv;
     // the same weights seen from the neighbour: per cone entry of c across face f, the neighbour's
     // LSQ state weight and aux weight for f (the transposed operators of the adjoint gather)
@@ -68,12 +68,37 @@ struct DevMesh {
     const double* cawr;
     int max_cone;
     // FP32 copies of the weights and offsets the mixed path rounds to FP32 anyway (identical results,
-    // half the bytes): cw, caw, cv and the tile-face offsets
-    const float* cw32;
-    const float* caw32;
+    // half the bytes): the packed weights (32-byte records, two floats of padding), cv and the
+    // tile-face offsets
+    const float* cwa32;
     const float* cv32;
     const float* tf_fdx32;
 };
+
+// state and aux weights of cone entry i in the reconstruction type G, from the packed record
+template <int DIM, class G>
+__device__ __forceinline__ void cone_weights(const double* __restrict__ p64, const float* __restrict__ p32, size_t i, G* w, G* a) {
+    if constexpr (std::is_same<G, float>::value) {
+        const float4 p = __ldg(reinterpret_cast<const float4*>(p32) + 2 * i);
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p32) + 2 * i + 1);
+        const float v[6] = {p.x, p.y, p.z, p.w, q.x, q.y};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            w[d] = v[d];
+            a[d] = v[3 + d];
+        }
+    } else {
+        const double2 p = __ldg(reinterpret_cast<const double2*>(p64) + 3 * i);
+        const double2 q = __ldg(reinterpret_cast<const double2*>(p64) + 3 * i + 1);
+        const double2 r = __ldg(reinterpret_cast<const double2*>(p64) + 3 * i + 2);
+        const double v[6] = {p.x, p.y, q.x, q.y, r.x, r.y};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+            w[d] = G(v[d]);
+            a[d] = G(v[3 + d]);
+        }
+    }
+}
 
 // a geometry value in the reconstruction type G: the FP32 copy for the mixed path
 template <class G>
@@ -354,10 +379,9 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) sd[((i - beg) * D::NC + k) * blockDim.x + threadIdx.x] = G(un[k] - uc[k]);
             }
+            G wd[DIM], wad[DIM];
+            cone_weights<DIM, G>(M.cwa, M.cwa32, (size_t)i, wd, wad);
             if (state && !(ce.y & kConeBoundary)) {
-                G wd[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = geo<G>(M.cw, M.cw32, 3 * (size_t)i + d);
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) {
                     const G delta = G(un[k] - uc[k]);
@@ -368,14 +392,11 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
             if (auxg) {
                 S an[D::NA];
                 cell_aux<DIM, NS>(P, un, aux, n, an);
-                G wd[DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) wd[d] = geo<G>(M.caw, M.caw32, 3 * (size_t)i + d);
 #pragma unroll
                 for (int k = 0; k < D::NA; k++) {
                     const G delta = G(an[k] - ac[k]);
 #pragma unroll
-                    for (int d = 0; d < DIM; d++) ga[k * DIM + d] += wd[d] * delta;
+                    for (int d = 0; d < DIM; d++) ga[k * DIM + d] += wad[d] * delta;
                 }
             }
         }
