@@ -460,8 +460,13 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                 }
             fv->cwa.upload(cwa.data(), cwa.size());
             fv->cv.upload(cv.data(), cv.size());
-            fv->cwr.upload(cwr.data(), cwr.size());
-            fv->cawr.upload(cawr.data(), cawr.size());
+            std::vector<double> cwar(6 * ncone);
+            for (size_t i = 0; i < ncone; i++)
+                for (int d = 0; d < 3; d++) {
+                    cwar[6 * i + d] = cwr[3 * i + d];
+                    cwar[6 * i + 3 + d] = cawr[3 * i + d];
+                }
+            fv->cwar.upload(cwar.data(), cwar.size());
             if (fv->ns == 0) {  // the mixed path's copies (with species it runs the FP64 kernels)
                 std::vector<float> f32(8 * ncone, 0.0f);
                 for (size_t i = 0; i < ncone; i++)
@@ -587,8 +592,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.wsum = fv->wsum.p;
         M.cwa = fv->cwa.p;
         M.cv = fv->cv.p;
-        M.cwr = fv->cwr.p;
-        M.cawr = fv->cawr.p;
+        M.cwar = fv->cwar.p;
         M.cwa32 = fv->cwa32.p;
         M.cv32 = fv->cv32.p;
         M.tf_fdx32 = fv->tf_fdx32.p;

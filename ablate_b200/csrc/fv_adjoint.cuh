@@ -936,11 +936,11 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
     for (int i = M.cone_ptr[m]; i < M.cone_ptr[m + 1]; i++) {
         const int2 ce = M.cone[i];
         const int f = ce.x, n = ce.y & kConeNbr;
+        double w[DIM], wa[DIM];
+        cone_weights<DIM, double>(M.cwar, nullptr, (size_t)i, w, wa);
         if (do_state) {
             if (!(ce.y & kConeBoundary)) {
-                double w[DIM], gn[D::NC * DIM];
-#pragma unroll
-                for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cwr + 3 * (size_t)i + d);
+                double gn[D::NC * DIM];
                 load_row<D::NC * DIM, double>(in.gb + (size_t)n * GR::GS, gn);
 #pragma unroll
                 for (int k = 0; k < D::NC; k++)
@@ -952,14 +952,12 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
                 if (__ldg(in.fstar + (size_t)n * D::NC + k) == f) ub[k] += __ldg(in.beta + (size_t)n * D::NC + k);
         }
         if (do_aux) {
-            double w[DIM], gn[D::NA * DIM];
-#pragma unroll
-            for (int d = 0; d < DIM; d++) w[d] = __ldg(M.cawr + 3 * (size_t)i + d);
+            double gn[D::NA * DIM];
             load_row<D::NA * DIM, double>(in.gab + (size_t)n * GR::AS, gn);
 #pragma unroll
             for (int k = 0; k < D::NA; k++)
 #pragma unroll
-                for (int d = 0; d < DIM; d++) ab[k] += w[d] * gn[k * DIM + d];
+                for (int d = 0; d < DIM; d++) ab[k] += wa[d] * gn[k * DIM + d];
         }
     }
     double u[D::NC];

@@ -103,7 +103,7 @@ struct abl_fv {
     // adjoint work buffers, allocated on the first VJP
     abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb, adj_graw, adj_phi;
     abl::DevBuf<int> adj_fstar, adj_ist;
-    abl::DevBuf<double> wsum, cwa, cv, cwr, cawr;
+    abl::DevBuf<double> wsum, cwa, cv, cwar;
     abl::DevBuf<float> cwa32, cv32, tf_fdx32;
     int max_cone = 0;
     // boundary ghosts and time stepping

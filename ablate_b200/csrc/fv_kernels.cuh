@@ -63,9 +63,9 @@ struct DevMesh {
     const double* cwa;
     const double* cv;
     // the same weights seen from the neighbour: per cone entry of c across face f, the neighbour's
-    // LSQ state weight and aux weight for f (the transposed operators of the adjoint gather)
-    const double* cwr;
-    const double* cawr;
+    // LSQ state weight and aux weight for f (the transposed operators of the adjoint gather), packed
+    // like cwa
+    const double* cwar;
     int max_cone;
     // FP32 copies of the weights and offsets the mixed path rounds to FP32 anyway (identical results,
     // half the bytes): the packed weights (32-byte records, two floats of padding), cv and the
