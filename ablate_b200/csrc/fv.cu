@@ -394,8 +394,27 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->tile_cells.upload(tl.cells.data(), tl.cells.size());
         fv->tile_face_ptr.upload(tl.face_ptr.data(), tl.face_ptr.size());
         fv->tf_cells.upload(reinterpret_cast<const int2*>(tl.tf_cells.data()), tl.tf_cells.size() / 2);
-        fv->tf_normal.upload(tl.tf_normal.data(), tl.tf_normal.size());
-        fv->tf_fdx.upload(tl.tf_fdx.data(), tl.tf_fdx.size());
+        {
+            // per tile face one 80-byte record: normal, both offsets, a pad (five 16-byte loads); the
+            // mixed path's 48-byte record holds the normal and the offsets as FP32 pairs
+            const size_t ntf = tl.tf_cells.size() / 2;
+            std::vector<double> geo(10 * ntf, 0.0);
+            for (size_t i = 0; i < ntf; i++) {
+                for (int d = 0; d < 3; d++) geo[10 * i + d] = tl.tf_normal[3 * i + d];
+                for (int z = 0; z < 6; z++) geo[10 * i + 3 + z] = tl.tf_fdx[6 * i + z];
+            }
+            fv->tf_geo.upload(geo.data(), geo.size());
+            if (fv->ns == 0) {
+                std::vector<double> g32(6 * ntf, 0.0);
+                for (size_t i = 0; i < ntf; i++) {
+                    for (int d = 0; d < 3; d++) g32[6 * i + d] = tl.tf_normal[3 * i + d];
+                    float f[6];
+                    for (int z = 0; z < 6; z++) f[z] = (float)tl.tf_fdx[6 * i + z];
+                    std::memcpy(&g32[6 * i + 3], f, sizeof f);
+                }
+                fv->tf_geo32.upload(g32.data(), g32.size());
+            }
+        }
         fv->tc_fptr.upload(tl.tc_fptr.data(), tl.tc_fptr.size());
         fv->tc_face.upload(tl.tc_face.data(), tl.tc_face.size());
         fv->col_base.upload(tl.col_base.data(), tl.col_base.size());
@@ -474,8 +493,6 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                 fv->cwa32.upload(f32.data(), f32.size());
                 f32.assign(cv.begin(), cv.end());
                 fv->cv32.upload(f32.data(), f32.size());
-                f32.assign(tl.tf_fdx.begin(), tl.tf_fdx.end());
-                fv->tf_fdx32.upload(f32.data(), f32.size());
             }
             fv->max_cone = maxc;
         }
@@ -577,8 +594,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.tile_cells = fv->tile_cells.p;
         M.tile_face_ptr = fv->tile_face_ptr.p;
         M.tf_cells = fv->tf_cells.p;
-        M.tf_normal = fv->tf_normal.p;
-        M.tf_fdx = fv->tf_fdx.p;
+        M.tf_geo = fv->tf_geo.p;
         M.tc_fptr = fv->tc_fptr.p;
         M.tc_face = fv->tc_face.p;
         M.tf_adj = fv->tf_adj.p;
@@ -595,7 +611,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.cwar = fv->cwar.p;
         M.cwa32 = fv->cwa32.p;
         M.cv32 = fv->cv32.p;
-        M.tf_fdx32 = fv->tf_fdx32.p;
+        M.tf_geo32 = fv->tf_geo32.p;
         M.max_cone = fv->max_cone;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();

@@ -878,9 +878,9 @@ __global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
             const int me = side ? lr.y : lr.x;
             double normal[DIM], fdxo[3];
 #pragma unroll
-            for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_normal + 3 * (size_t)i + d);
+            for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_geo + 10 * (size_t)i + d);
 #pragma unroll
-            for (int d = 0; d < 3; d++) fdxo[d] = __ldg(M.tf_fdx + 6 * (size_t)i + 3 * side + d);
+            for (int d = 0; d < 3; d++) fdxo[d] = __ldg(M.tf_geo + 10 * (size_t)i + 3 + 3 * side + d);
             // destination: this tile's accumulator, the record of a non-owned side, or none
             const uint32_t slots = M.tf_slot[i];
             const int slot = side ? int(slots >> 16) : int(slots & 0xffff);

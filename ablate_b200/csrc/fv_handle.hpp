@@ -82,7 +82,7 @@ struct abl_fv {
     // tiles
     abl::DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
     abl::DevBuf<int2> tf_cells;
-    abl::DevBuf<double> tf_normal, tf_fdx;
+    abl::DevBuf<double> tf_geo, tf_geo32;
     abl::DevBuf<uint16_t> tc_face;
     int tile_smem = 0;
     // adjoint: tile face colours and slots, non-owned records
@@ -104,7 +104,7 @@ struct abl_fv {
     abl::DevBuf<double> adj_gb, adj_beta, adj_gab, adj_ub, adj_ab, adj_nb, adj_graw, adj_phi;
     abl::DevBuf<int> adj_fstar, adj_ist;
     abl::DevBuf<double> wsum, cwa, cv, cwar;
-    abl::DevBuf<float> cwa32, cv32, tf_fdx32;
+    abl::DevBuf<float> cwa32, cv32;
     int max_cone = 0;
     // boundary ghosts and time stepping
     int n_ghost = 0;

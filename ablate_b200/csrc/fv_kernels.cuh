@@ -43,8 +43,7 @@ struct DevMesh {
     const int* tile_cells;
     const int* tile_face_ptr;
     const int2* tf_cells;
-    const double* tf_normal;  // [ntf][3]
-    const double* tf_fdx;     // [ntf][6]
+    const double* tf_geo;     // [ntf][10]: area normal (3), face centroid minus each side's centroid (6), pad
     const int* tc_fptr;
     const uint16_t* tc_face;
     // adjoint: face colours per tile, tile-local slots, records of faces with a non-owned side
@@ -72,7 +71,7 @@ struct DevMesh {
     // tile-face offsets
     const float* cwa32;
     const float* cv32;
-    const float* tf_fdx32;
+    const double* tf_geo32;   // [ntf][6]: the area normal (3 doubles), then the 6 offsets as FP32 pairs (mixed path)
 };
 
 // state and aux weights of cone entry i in the reconstruction type G, from the packed record
@@ -719,6 +718,38 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 }
 
 // ---------------------------------------------------------------------------------------------------
+// area normal and both sides' offsets of tile face i with vector loads of its geometry record
+template <int DIM, class G>
+__device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* normal, double* fdx) {
+    if constexpr (std::is_same<G, float>::value) {
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo32) + 3 * (size_t)i;
+        const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
+        const double n[3] = {a.x, a.y, b.x};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) normal[d] = n[d];
+        const double packed[3] = {b.y, c.x, c.y};
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(packed[q]);
+            fdx[2 * q] = double(__int_as_float((int)(bits & 0xffffffffull)));
+            fdx[2 * q + 1] = double(__int_as_float((int)(bits >> 32)));
+        }
+    } else {
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo) + 5 * (size_t)i;
+        const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), e = __ldg(r + 3), f = __ldg(r + 4);
+        const double n[3] = {a.x, a.y, b.x};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) normal[d] = n[d];
+        fdx[0] = b.y;
+        fdx[1] = c.x;
+        fdx[2] = c.y;
+        fdx[3] = e.x;
+        fdx[4] = e.y;
+        fdx[5] = f.x;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
 // One CTA per tile. Phase 1: face fluxes into shared memory (tile-ordered geometry streamed from HBM).
 // Phase 2: each tile cell adds -+flux/V of its faces in ascending face order and writes F once.
 template <int DIM, int NS, class G, int FK>
@@ -737,13 +768,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
     for (int i = fb + threadIdx.x; i < fe; i += blockDim.x) {
         const int2 lr = M.tf_cells[i];
         double normal[DIM], fdx[6];
-#pragma unroll
-        for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_normal + 3 * (size_t)i + d);
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            fdx[d] = std::is_same<G, float>::value ? double(__ldg(M.tf_fdx32 + 6 * (size_t)i + d)) : __ldg(M.tf_fdx + 6 * (size_t)i + d);
-            fdx[3 + d] = std::is_same<G, float>::value ? double(__ldg(M.tf_fdx32 + 6 * (size_t)i + 3 + d)) : __ldg(M.tf_fdx + 6 * (size_t)i + 3 + d);
-        }
+        face_geometry<DIM, G>(M, i, normal, fdx);
         S flux[D::NC];
         face_flux<DIM, NS, G, FK>(M, P, lr.x, lr.y, normal, fdx, U, dU, aux, grad, agrad, flux, &ok, &rok);
         S* out = sflux + (size_t)(i - fb) * D::NC;
