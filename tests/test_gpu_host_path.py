@@ -1,7 +1,7 @@
 """The host-buffer RHS (abl_fv_rhs_host: the state and the residual copied in, the residual added to
 and copied out, with the residual's copies overlapped with the kernels) against the device-pointer RHS,
-bit for bit, on meshes whose tiles are contiguous cell ranges (copied out tile chunk by tile chunk) and
-on one whose tiles are not."""
+bit for bit: on a mesh whose residual is large enough to travel in tile chunks, on small ones, with
+ghost rows, and on one whose tiles are not cell ranges."""
 import numpy as np
 import pytest
 
@@ -13,20 +13,22 @@ from tests import rhs_cases as R
 pytestmark = pytest.mark.gpu
 
 
-def _cases():
-    w1 = workloads.tgv3d(16)                       # 16 tiles, Morton-numbered cells: chunked copies
+def _cases(name):
+    if name == "tgv76":
+        return workloads.tgv3d(76)                 # 17.6 MB residual, Morton-numbered cells: chunked copies
+    w1 = workloads.tgv3d(16)                       # small residual: one copy each way
     w2 = workloads.wall3d(12)                      # ghosts after the owned rows
     w3 = workloads.tgv3d(12)
     w3.mesh = box_mesh((12, 12, 12), periodic=(True, True, True), order="natural")
     w3.U = workloads.tgv_state(w3.mesh)            # natural numbering: tiles are not ranges
-    return {"tgv16": w1, "wall12": w2, "tgv12_natural": w3, "species": R.case("species3d_ns5")}
+    return {"tgv16": w1, "wall12": w2, "tgv12_natural": w3, "species": R.case("species3d_ns5")}[name]
 
 
-@pytest.mark.parametrize("name", ["tgv16", "wall12", "tgv12_natural", "species"])
+@pytest.mark.parametrize("name", ["tgv76", "tgv16", "wall12", "tgv12_natural", "species"])
 @pytest.mark.parametrize("precision", [L.PRECISION_FP64, L.PRECISION_MIXED])
 def test_host_path_adds_the_device_residual(name, precision):
     torch = pytest.importorskip("torch")
-    w = _cases()[name]
+    w = _cases(name)
     s = w.solver()
     rng = np.random.default_rng(4)
     F0 = rng.standard_normal(w.U.shape)
