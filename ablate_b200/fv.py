@@ -18,7 +18,6 @@ implementation in this package.
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
 from typing import Sequence
 
 import numpy as np
