@@ -77,6 +77,7 @@ SIGNATURES = {
     "abl_fv_create": (C.c_int, [C.POINTER(MeshDesc), C.POINTER(PhysicsDesc), C.c_int, C.POINTER(C.c_void_p)]),
     "abl_fv_destroy": (C.c_int, [C.c_void_p]),
     "abl_fv_sizes": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
+    "abl_fv_record_classes": (C.c_int, [C.c_void_p, _ip, _ip]),
     "abl_fv_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
     "abl_fv_jvp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

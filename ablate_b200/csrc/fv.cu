@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -22,6 +23,13 @@ thread_local std::string g_last_error;
 using namespace abl;
 
 namespace {
+
+// repeated geometry and weight records stored once (the default); ABL_FV_RECORD_TABLES=0 keeps one
+// record per face and cone entry
+bool record_tables() {
+    const char* v = std::getenv("ABL_FV_RECORD_TABLES");
+    return !(v && v[0] == '0');
+}
 
 int fail(const AblError& e) {
     g_last_error = e.what();
@@ -397,19 +405,36 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         {
             // per tile face one 80-byte record: normal, both offsets, a pad (five 16-byte loads); the
             // mixed path's 48-byte record holds the normal and the offsets as FP32 pairs
-            const size_t ntf = tl.tf_cells.size() / 2;
+            size_t ntf = tl.tf_cells.size() / 2;
             std::vector<double> geo(10 * ntf, 0.0);
             for (size_t i = 0; i < ntf; i++) {
                 for (int d = 0; d < 3; d++) geo[10 * i + d] = tl.tf_normal[3 * i + d];
                 for (int z = 0; z < 6; z++) geo[10 * i + 3 + z] = tl.tf_fdx[6 * i + z];
             }
+            if (record_tables() && ntf >= 8) {
+                // records that repeat bit for bit (the faces of a structured block) are stored once
+                std::vector<int32_t> cls;
+                std::vector<size_t> rep;
+                const size_t ng = abl::distinct_classes(
+                    ntf, std::min(abl::kMaxRecordClasses, ntf / 8), [&](size_t k) { return abl::hash_bits(&geo[10 * k], 10); },
+                    [&](size_t a, size_t b) { return std::memcmp(&geo[10 * a], &geo[10 * b], 10 * sizeof(double)) == 0; }, cls, rep);
+                if (ng) {
+                    std::vector<double> table(10 * ng);
+                    for (size_t j = 0; j < ng; j++) std::copy_n(&geo[10 * rep[j]], 10, &table[10 * j]);
+                    std::vector<uint16_t> c16(cls.begin(), cls.end());
+                    fv->tf_gcls.upload(c16.data(), c16.size());
+                    fv->n_geo_classes = (int)ng;
+                    geo.swap(table);
+                    ntf = ng;
+                }
+            }
             fv->tf_geo.upload(geo.data(), geo.size());
             if (fv->ns == 0) {
                 std::vector<double> g32(6 * ntf, 0.0);
                 for (size_t i = 0; i < ntf; i++) {
-                    for (int d = 0; d < 3; d++) g32[6 * i + d] = tl.tf_normal[3 * i + d];
+                    for (int d = 0; d < 3; d++) g32[6 * i + d] = geo[10 * i + d];
                     float f[6];
-                    for (int z = 0; z < 6; z++) f[z] = (float)tl.tf_fdx[6 * i + z];
+                    for (int z = 0; z < 6; z++) f[z] = (float)geo[10 * i + 3 + z];
                     std::memcpy(&g32[6 * i + 3], f, sizeof f);
                 }
                 fv->tf_geo32.upload(g32.data(), g32.size());
@@ -480,18 +505,57 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                     cwa[6 * i + d] = cw[3 * i + d];
                     cwa[6 * i + 3 + d] = caw[3 * i + d];
                 }
-            fv->cwa.upload(cwa.data(), cwa.size());
-            fv->cv.upload(cv.data(), cv.size());
             std::vector<double> cwar(6 * ncone);
             for (size_t i = 0; i < ncone; i++)
                 for (int d = 0; d < 3; d++) {
                     cwar[6 * i + d] = cwr[3 * i + d];
                     cwar[6 * i + 3 + d] = cawr[3 * i + d];
                 }
+            if (record_tables() && h.n_cells >= 8) {
+                // cells whose weight sequences (cwa, cv, cwar over the cone) repeat bit for bit (the
+                // cells of a structured block) share one copy
+                auto seq_hash = [&](size_t c) {
+                    const size_t b = (size_t)h.cone_ptr[c], n = (size_t)h.cone_ptr[c + 1] - b;
+                    uint64_t hh = abl::hash_bits(&cwa[6 * b], 6 * n);
+                    hh = abl::hash_bits(&cv[3 * b], 3 * n, hh);
+                    return abl::hash_bits(&cwar[6 * b], 6 * n, hh);
+                };
+                auto seq_same = [&](size_t a, size_t c) {
+                    const size_t ba = (size_t)h.cone_ptr[a], na = (size_t)h.cone_ptr[a + 1] - ba;
+                    const size_t bc = (size_t)h.cone_ptr[c], nn = (size_t)h.cone_ptr[c + 1] - bc;
+                    return na == nn && std::memcmp(&cwa[6 * ba], &cwa[6 * bc], 6 * nn * sizeof(double)) == 0 &&
+                           std::memcmp(&cv[3 * ba], &cv[3 * bc], 3 * nn * sizeof(double)) == 0 &&
+                           std::memcmp(&cwar[6 * ba], &cwar[6 * bc], 6 * nn * sizeof(double)) == 0;
+                };
+                std::vector<int32_t> cls;
+                std::vector<size_t> rep;
+                const size_t ncl = abl::distinct_classes((size_t)h.n_cells, std::min(abl::kMaxRecordClasses, (size_t)h.n_cells / 8),
+                                                         seq_hash, seq_same, cls, rep);
+                if (ncl) {
+                    std::vector<int32_t> start(ncl + 1, 0), base(h.n_cells);
+                    for (size_t j = 0; j < ncl; j++) start[j + 1] = start[j] + h.cone_ptr[rep[j] + 1] - h.cone_ptr[rep[j]];
+                    std::vector<double> tw(6 * (size_t)start[ncl]), tv(3 * (size_t)start[ncl]), twr(6 * (size_t)start[ncl]);
+                    for (size_t j = 0; j < ncl; j++) {
+                        const size_t b = (size_t)h.cone_ptr[rep[j]], n = (size_t)(start[j + 1] - start[j]), o = (size_t)start[j];
+                        std::copy_n(&cwa[6 * b], 6 * n, &tw[6 * o]);
+                        std::copy_n(&cv[3 * b], 3 * n, &tv[3 * o]);
+                        std::copy_n(&cwar[6 * b], 6 * n, &twr[6 * o]);
+                    }
+                    for (int c = 0; c < h.n_cells; c++) base[c] = start[cls[c]];
+                    cwa.swap(tw);
+                    cv.swap(tv);
+                    cwar.swap(twr);
+                    fv->cone_cls.upload(base.data(), base.size());
+                    fv->n_cone_classes = (int)ncl;
+                }
+            }
+            fv->cwa.upload(cwa.data(), cwa.size());
+            fv->cv.upload(cv.data(), cv.size());
             fv->cwar.upload(cwar.data(), cwar.size());
             if (fv->ns == 0) {  // the mixed path's copies (with species it runs the FP64 kernels)
-                std::vector<float> f32(8 * ncone, 0.0f);
-                for (size_t i = 0; i < ncone; i++)
+                const size_t nw = cwa.size() / 6;
+                std::vector<float> f32(8 * nw, 0.0f);
+                for (size_t i = 0; i < nw; i++)
                     for (int d = 0; d < 6; d++) f32[8 * i + d] = (float)cwa[6 * i + d];
                 fv->cwa32.upload(f32.data(), f32.size());
                 f32.assign(cv.begin(), cv.end());
@@ -615,6 +679,8 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         M.cwa32 = fv->cwa32.p;
         M.cv32 = fv->cv32.p;
         M.tf_geo32 = fv->tf_geo32.p;
+        M.cone_cls = fv->n_cone_classes ? fv->cone_cls.p : nullptr;
+        M.tf_gcls = fv->n_geo_classes ? fv->tf_gcls.p : nullptr;
         M.max_cone = fv->max_cone;
         ABL_CUDA(cudaDeviceSynchronize());
         *out = fv.release();
@@ -666,6 +732,13 @@ int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells,
     if (naux) *naux = fv->naux;
     if (n_cells) *n_cells = fv->n_cells;
     if (n_faces) *n_faces = fv->n_faces;
+    return ABL_OK;
+}
+
+int abl_fv_record_classes(const abl_fv* fv, int32_t* weight_classes, int32_t* geometry_classes) {
+    if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (weight_classes) *weight_classes = fv->n_cone_classes;
+    if (geometry_classes) *geometry_classes = fv->n_geo_classes;
     return ABL_OK;
 }
 

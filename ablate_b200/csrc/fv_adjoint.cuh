@@ -877,10 +877,11 @@ __global__ void __launch_bounds__(256, AdjBlocks<NS>::tile) k_tile_adjoint(DevMe
             const int2 lr = M.tf_cells[i];
             const int me = side ? lr.y : lr.x;
             double normal[DIM], fdxo[3];
+            const double* geo = M.tf_geo + 10 * geo_record(M, i);
 #pragma unroll
-            for (int d = 0; d < DIM; d++) normal[d] = __ldg(M.tf_geo + 10 * (size_t)i + d);
+            for (int d = 0; d < DIM; d++) normal[d] = __ldg(geo + d);
 #pragma unroll
-            for (int d = 0; d < 3; d++) fdxo[d] = __ldg(M.tf_geo + 10 * (size_t)i + 3 + 3 * side + d);
+            for (int d = 0; d < 3; d++) fdxo[d] = __ldg(geo + 3 + 3 * side + d);
             // destination: this tile's accumulator, the record of a non-owned side, or none
             const uint32_t slots = M.tf_slot[i];
             const int slot = side ? int(slots >> 16) : int(slots & 0xffff);
@@ -932,12 +933,14 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
     for (int k = 0; k < D::NC; k++) ub[k] = in.ub[(size_t)m * D::NC + k];
 #pragma unroll
     for (int k = 0; k < D::NA; k++) ab[k] = in.ab[(size_t)m * D::NA + k];
+    const int beg = M.cone_ptr[m];
+    const size_t wb = weight_base(M, m, beg);
 #pragma unroll 1
-    for (int i = M.cone_ptr[m]; i < M.cone_ptr[m + 1]; i++) {
+    for (int i = beg; i < M.cone_ptr[m + 1]; i++) {
         const int2 ce = M.cone[i];
         const int f = ce.x, n = ce.y & kConeNbr;
         double w[DIM], wa[DIM];
-        cone_weights<DIM, double>(M.cwar, nullptr, (size_t)i, w, wa);
+        cone_weights<DIM, double>(M.cwar, nullptr, wb + (size_t)(i - beg), w, wa);
         if (do_state) {
             if (!(ce.y & kConeBoundary)) {
                 double gn[D::NC * DIM];

@@ -83,6 +83,8 @@ struct abl_fv {
     abl::DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
     abl::DevBuf<int2> tf_cells;
     abl::DevBuf<double> tf_geo, tf_geo32;
+    abl::DevBuf<uint16_t> tf_gcls;  // per tile face record, its geometry record (when they repeat)
+    int n_geo_classes = 0;          // 0: one geometry record per tile face record
     abl::DevBuf<uint16_t> tc_face;
     int tile_smem = 0;
     // adjoint: tile face colours and slots, non-owned records
@@ -105,6 +107,8 @@ struct abl_fv {
     abl::DevBuf<int> adj_fstar, adj_ist;
     abl::DevBuf<double> wsum, cwa, cv, cwar;
     abl::DevBuf<float> cwa32, cv32;
+    abl::DevBuf<int> cone_cls;  // per cell, the first entry of its weight sequence (when they repeat)
+    int n_cone_classes = 0;     // 0: one weight record per cone entry
     int max_cone = 0;
     // boundary ghosts and time stepping
     int n_ghost = 0;

@@ -72,7 +72,22 @@ struct DevMesh {
     const float* cwa32;
     const float* cv32;
     const double* tf_geo32;   // [ntf][6]: the area normal (3 doubles), then the 6 offsets as FP32 pairs (mixed path)
+    // When records repeat bit for bit (a structured block), tf_geo / tf_geo32 hold one record per
+    // distinct one and tf_gcls gives each tile face record its copy; likewise cwa, cv, cwar (and their
+    // FP32 copies) hold one weight sequence per distinct cell cone and cone_cls gives each cell the
+    // first entry of its copy. Null: one record per face / cone entry.
+    const uint16_t* tf_gcls;
+    const int* cone_cls;
 };
+
+// the first weight record of cell c, whose cone starts at entry beg
+__device__ __forceinline__ size_t weight_base(const DevMesh& M, int c, int beg) {
+    return M.cone_cls ? (size_t)__ldg(M.cone_cls + c) : (size_t)beg;
+}
+// the geometry record of tile face record i
+__device__ __forceinline__ size_t geo_record(const DevMesh& M, int i) {
+    return M.tf_gcls ? (size_t)__ldg(M.tf_gcls + i) : (size_t)i;
+}
 
 // state and aux weights of cone entry i in the reconstruction type G, from the packed record
 template <int DIM, class G>
@@ -269,7 +284,7 @@ __global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __
 // sd, when not null, holds the cell's neighbour differences u_n - u_c per cone entry (written by the
 // gradient pass; thread-interleaved) so the neighbour states are not read again.
 template <int DIM, int NS, class G, int LIM, bool REC = false>
-__device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, const double* __restrict__ U,
+__device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int beg, int end, size_t wb, const double* __restrict__ U,
                                             const double* __restrict__ dU, const StateOf<G>* uc, G* g, int k0, int k1,
                                             double* rphi = nullptr, int* rist = nullptr, const G* sd = nullptr) {
     using D = Dims<DIM, NS>;
@@ -286,7 +301,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
         // x_n - x_c, periodic images resolved (face offsets taken in each cell's own frame)
         G v[DIM];
 #pragma unroll
-        for (int d = 0; d < DIM; d++) v[d] = geo<G>(M.cv, M.cv32, 3 * (size_t)i + d);
+        for (int d = 0; d < DIM; d++) v[d] = geo<G>(M.cv, M.cv32, 3 * (wb + (size_t)(i - beg)) + d);
         S un[D::NC];
         if (!sd) load_state<DIM, NS, S>(U, dU, M.cone[i].y & kConeNbr, un);
 #pragma unroll
@@ -354,6 +369,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
     if (c >= M.n_cells) return;
     const uint8_t kind = M.kind[c];
     const int beg = M.cone_ptr[c], end = M.cone_ptr[c + 1];
+    const size_t wb = weight_base(M, c, beg);
     const bool state = do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO);
     const bool auxg = do_aux && kind != ABL_CELL_HALO_OUTER;
     const bool nasa = NS > 0 && P.eos == ABL_EOS_NASA7;
@@ -379,7 +395,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 for (int k = 0; k < D::NC; k++) sd[((i - beg) * D::NC + k) * blockDim.x + threadIdx.x] = G(un[k] - uc[k]);
             }
             G wd[DIM], wad[DIM];
-            cone_weights<DIM, G>(M.cwa, M.cwa32, (size_t)i, wd, wad);
+            cone_weights<DIM, G>(M.cwa, M.cwa32, wb + (size_t)(i - beg), wd, wad);
             if (state && !(ce.y & kConeBoundary)) {
 #pragma unroll
                 for (int k = 0; k < D::NC; k++) {
@@ -414,8 +430,8 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 for (int k = 0; k < D::NC * DIM; k++) o[k] = g[k];
             }
             if (state && P.limiter != ABL_LIMITER_NONE) {
-                limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, 0, D::NE, ph, is, sd);
-                if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, ph, is, sd);
+                limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, wb, U, dU, uc, g, 0, D::NE, ph, is, sd);
+                if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, wb, U, dU, uc, g, D::NE, D::NC, ph, is, sd);
             }
             if (do_state) {
 #pragma unroll
@@ -425,8 +441,8 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 }
             }
         } else if (state && P.limiter != ABL_LIMITER_NONE) {
-            limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, 0, D::NE, nullptr, nullptr, sd);
-            if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, U, dU, uc, g, D::NE, D::NC, nullptr, nullptr, sd);
+            limit_field<DIM, NS, G, LIM>(M, P, beg, end, wb, U, dU, uc, g, 0, D::NE, nullptr, nullptr, sd);
+            if (NS > 0) limit_field<DIM, NS, G, LIM>(M, P, beg, end, wb, U, dU, uc, g, D::NE, D::NC, nullptr, nullptr, sd);
         }
     }
     if (do_state) {
@@ -722,7 +738,7 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 template <int DIM, class G>
 __device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* normal, double* fdx) {
     if constexpr (std::is_same<G, float>::value) {
-        const double2* r = reinterpret_cast<const double2*>(M.tf_geo32) + 3 * (size_t)i;
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo32) + 3 * geo_record(M, i);
         const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
         const double n[3] = {a.x, a.y, b.x};
 #pragma unroll
@@ -735,7 +751,7 @@ __device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* n
             fdx[2 * q + 1] = double(__int_as_float((int)(bits >> 32)));
         }
     } else {
-        const double2* r = reinterpret_cast<const double2*>(M.tf_geo) + 5 * (size_t)i;
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo) + 5 * geo_record(M, i);
         const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), e = __ldg(r + 3), f = __ldg(r + 4);
         const double n[3] = {a.x, a.y, b.x};
 #pragma unroll

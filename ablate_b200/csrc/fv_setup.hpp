@@ -13,10 +13,13 @@
 #pragma once
 #include "fv_consts.hpp"
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/ablate_fv.h"
@@ -28,7 +31,7 @@ struct HostMesh {
     std::vector<int32_t> face_cells;     // [nf][2]
     std::vector<uint8_t> kind;           // [nc]
     std::vector<int32_t> cone_ptr;       // [nc+1]
-    std::vector<int32_t> cone_face;      // faces of each cell, ascending
+    std::vector<int32_t> cone_face;      // faces of each cell, by neighbour offset (canonical order)
     std::vector<int32_t> cone_nbr;       // neighbour across that face
     std::vector<uint8_t> cone_side;      // 0: the cell is the face's left cell
     std::vector<uint8_t> face_boundary;  // a boundary ghost cell is on one side
@@ -413,6 +416,39 @@ inline HostMesh build_host_mesh(const abl_mesh_desc* m, bool need_cgrad, bool ne
         const double xn = m->cell_centroid[3 * (size_t)n + d] + (h.cone_side[i] == 0 ? sh : -sh);
         return xn - m->cell_centroid[3 * (size_t)c + d];
     };
+    // each cell's cone in one canonical order: by the neighbour offset x_n - x_c (lexicographic), then
+    // by face index. The cells of a structured block then list their neighbours alike and get bitwise
+    // the same least-squares weights, and cone entry i points the same way for neighbouring cells.
+    {
+        std::vector<std::pair<std::array<double, 3>, int>> key;
+        std::vector<int32_t> cf, cn;
+        std::vector<uint8_t> cs;
+        for (int c = 0; c < nc; c++) {
+            const int b = h.cone_ptr[c], n = h.cone_ptr[c + 1] - b;
+            if (n < 2) continue;
+            key.clear();
+            for (int i = b; i < b + n; i++) {
+                std::array<double, 3> v{0.0, 0.0, 0.0};
+                for (int d = 0; d < dim; d++) v[d] = nbr_dx(c, i, d);
+                key.push_back({v, i});
+            }
+            std::sort(key.begin(), key.end(), [&](const auto& x, const auto& y) {
+                if (x.first != y.first) return x.first < y.first;
+                return h.cone_face[x.second] < h.cone_face[y.second];
+            });
+            cf.resize(n);
+            cn.resize(n);
+            cs.resize(n);
+            for (int k = 0; k < n; k++) {
+                cf[k] = h.cone_face[key[k].second];
+                cn[k] = h.cone_nbr[key[k].second];
+                cs[k] = h.cone_side[key[k].second];
+            }
+            std::copy(cf.begin(), cf.end(), h.cone_face.begin() + b);
+            std::copy(cn.begin(), cn.end(), h.cone_nbr.begin() + b);
+            std::copy(cs.begin(), cs.end(), h.cone_side.begin() + b);
+        }
+    }
     std::vector<double> B, W;
     if (need_cgrad) {
         h.cgrad.assign((size_t)nf * 6, 0.0);
@@ -451,5 +487,46 @@ inline HostMesh build_host_mesh(const abl_mesh_desc* m, bool need_cgrad, bool ne
     }
     return h;
 }
+
+// Classes of n items that are equal bit for bit: hash(k) gives item k's hash, same(a, b) compares two
+// items. Fills cls[k] with item k's class (classes numbered in order of first appearance) and rep[j]
+// with the first item of class j, and returns the number of classes; returns 0 as soon as there are
+// more than max_cls.
+template <class Hash, class Same>
+inline size_t distinct_classes(size_t n, size_t max_cls, Hash hash, Same same, std::vector<int32_t>& cls, std::vector<size_t>& rep) {
+    std::unordered_multimap<uint64_t, int32_t> seen;
+    cls.assign(n, -1);
+    rep.clear();
+    for (size_t k = 0; k < n; k++) {
+        const uint64_t hk = hash(k);
+        const auto range = seen.equal_range(hk);
+        for (auto it = range.first; it != range.second; ++it)
+            if (same(rep[(size_t)it->second], k)) {
+                cls[k] = it->second;
+                break;
+            }
+        if (cls[k] >= 0) continue;
+        if (rep.size() == max_cls) return 0;
+        cls[k] = (int32_t)rep.size();
+        seen.emplace(hk, cls[k]);
+        rep.push_back(k);
+    }
+    return rep.size();
+}
+
+// a hash of the bits of n doubles, continuing from h: per word, xor, multiply by the 64-bit FNV prime
+// and fold the high bits down
+inline uint64_t hash_bits(const double* p, size_t n, uint64_t h = 1469598103934665603ull) {
+    for (size_t i = 0; i < n; i++) {
+        uint64_t b;
+        std::memcpy(&b, p + i, sizeof b);
+        h = (h ^ b) * 1099511628211ull;
+        h ^= h >> 29;
+    }
+    return h;
+}
+
+// Record tables are used when the distinct records are at most this many and at most 1/8 of the items.
+constexpr size_t kMaxRecordClasses = 4096;
 
 }  // namespace abl

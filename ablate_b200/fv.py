@@ -509,6 +509,13 @@ class FiniteVolumeSolver:
         L.check(L.lib.abl_fv_launch_count(self.handle, precision, C.byref(n)))
         return n.value
 
+    def RecordClasses(self) -> tuple[int, int]:
+        """(weight classes, geometry classes) of the device layout: the distinct per-cell cone weight
+        sequences and tile face geometry records stored once, 0 where every cell / face has its own."""
+        w, g = C.c_int32(), C.c_int32()
+        L.check(L.lib.abl_fv_record_classes(self.handle, C.byref(w), C.byref(g)))
+        return w.value, g.value
+
     def close(self):
         if getattr(self, "handle", None):
             L.lib.abl_fv_destroy(self.handle)

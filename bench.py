@@ -538,7 +538,8 @@ def main():
         "config": {"workload": w.name, "n_cells": world * n_cells, "cells_per_gpu": n_cells, "n_faces": int(w.mesh.n_faces), "description": w.description,
                    "parallelism": (f"dp{world}: x-slab partition, 2-layer halo exchanged over NCCL point-to-point before every RHS "
                                    f"({drhs.halo.bytes_per_exchange} B per rank per step)") if world > 1 else "single GPU",
-                   "l2": "flushed (256 MiB write) between timed steps, outside the timed events"},
+                   "l2": "flushed (256 MiB write) between timed steps, outside the timed events",
+                   "record_classes": dict(zip(("cone_weights", "face_geometry"), solver.RecordClasses()))},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_achieved, "peak": peak, "unit": "GB/s", "frac": dom_achieved / peak,
                      "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed", dom_name, n_cells) if world == 1 else None,
                      "algorithmic_bytes_per_launch": B, "kernel_ms": dom_ms,

@@ -170,6 +170,13 @@ int abl_device_count(int* count);
 int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, int device, abl_fv** out);
 int abl_fv_destroy(abl_fv* fv);
 int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells, int32_t* n_faces);
+/* The device layout abl_fv_create chose (no reference counterpart: PETSc stores one geometry record per
+ * face and one weight set per cell). Tile face geometry records and per-cell cone weight sequences that
+ * repeat bit for bit (a structured block) are stored once and read through a per-face / per-cell index
+ * when there are at most 4096 distinct ones and at most 1/8 of the records; results are bitwise the
+ * same. 0 = one record per face / cone entry. The environment variable ABL_FV_RECORD_TABLES=0, read at
+ * create, keeps one record per face and cone entry. */
+int abl_fv_record_classes(const abl_fv* fv, int32_t* weight_classes, int32_t* geometry_classes);
 
 /* ---- the hot path ----------------------------------------------------------------------------- */
 /* F += RHS(U) for owned cells, device pointers, on `stream` (a cudaStream_t; NULL = legacy stream).
