@@ -403,30 +403,15 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->tile_face_ptr.upload(tl.face_ptr.data(), tl.face_ptr.size());
         fv->tf_cells.upload(reinterpret_cast<const int2*>(tl.tf_cells.data()), tl.tf_cells.size() / 2);
         {
-            // per tile face one 80-byte record: normal, both offsets, a pad (five 16-byte loads); the
-            // mixed path's 48-byte record holds the normal and the offsets as FP32 pairs
-            size_t ntf = tl.tf_cells.size() / 2;
-            std::vector<double> geo(10 * ntf, 0.0);
-            for (size_t i = 0; i < ntf; i++) {
-                for (int d = 0; d < 3; d++) geo[10 * i + d] = tl.tf_normal[3 * i + d];
-                for (int z = 0; z < 6; z++) geo[10 * i + 3 + z] = tl.tf_fdx[6 * i + z];
-            }
-            if (record_tables() && ntf >= 8) {
-                // records that repeat bit for bit (the faces of a structured block) are stored once
-                std::vector<int32_t> cls;
-                std::vector<size_t> rep;
-                const size_t ng = abl::distinct_classes(
-                    ntf, std::min(abl::kMaxRecordClasses, ntf / 8), [&](size_t k) { return abl::hash_bits(&geo[10 * k], 10); },
-                    [&](size_t a, size_t b) { return std::memcmp(&geo[10 * a], &geo[10 * b], 10 * sizeof(double)) == 0; }, cls, rep);
-                if (ng) {
-                    std::vector<double> table(10 * ng);
-                    for (size_t j = 0; j < ng; j++) std::copy_n(&geo[10 * rep[j]], 10, &table[10 * j]);
-                    std::vector<uint16_t> c16(cls.begin(), cls.end());
-                    fv->tf_gcls.upload(c16.data(), c16.size());
-                    fv->n_geo_classes = (int)ng;
-                    geo.swap(table);
-                    ntf = ng;
-                }
+            // per tile face one 80-byte record: normal, both offsets, a pad (five 16-byte loads), stored
+            // once per distinct record where they repeat; the mixed path's 48-byte record holds the
+            // normal and the offsets as FP32 pairs
+            GeoRecords gr = tile_geometry(tl, record_tables());
+            const std::vector<double>& geo = gr.geo;
+            const size_t ntf = geo.size() / 10;
+            if (!gr.cls.empty()) {
+                fv->tf_gcls.upload(gr.cls.data(), gr.cls.size());
+                fv->n_geo_classes = (int)ntf;
             }
             fv->tf_geo.upload(geo.data(), geo.size());
             if (fv->ns == 0) {
@@ -477,77 +462,15 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         if (lsq) fv->cgrad.upload(h.cgrad.data(), h.cgrad.size());
         if (dif) fv->fgrad.upload(h.fgrad.data(), h.fgrad.size());
         {
-            // cone-major geometry: per cone entry the LSQ state weight (0 across boundary faces and for
-            // cells without a state gradient), the aux weight and the neighbour offset x_n - x_c
-            const size_t ncone = h.cone_face.size();
-            std::vector<double> cw(3 * ncone, 0.0), caw(3 * ncone, 0.0), cv(3 * ncone, 0.0), cwr(3 * ncone, 0.0), cawr(3 * ncone, 0.0);
-            int maxc = 0;
-            for (int c = 0; c < h.n_cells; c++) {
-                maxc = std::max(maxc, h.cone_ptr[c + 1] - h.cone_ptr[c]);
-                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
-                    const int f = h.cone_face[i], sc = h.cone_side[i];
-                    for (int d = 0; d < 3; d++) {
-                        if (lsq && !h.face_boundary[f]) {
-                            cw[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * sc + d];
-                            cwr[3 * (size_t)i + d] = h.cgrad[6 * (size_t)f + 3 * (1 - sc) + d];
-                        }
-                        if (dif) {
-                            caw[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * sc + d];
-                            cawr[3 * (size_t)i + d] = h.fgrad[6 * (size_t)f + 3 * (1 - sc) + d];
-                        }
-                        cv[3 * (size_t)i + d] = h.fdx[6 * (size_t)f + 3 * sc + d] - h.fdx[6 * (size_t)f + 3 * (1 - sc) + d];
-                    }
-                }
-            }
-            std::vector<double> cwa(6 * ncone);
-            for (size_t i = 0; i < ncone; i++)
-                for (int d = 0; d < 3; d++) {
-                    cwa[6 * i + d] = cw[3 * i + d];
-                    cwa[6 * i + 3 + d] = caw[3 * i + d];
-                }
-            std::vector<double> cwar(6 * ncone);
-            for (size_t i = 0; i < ncone; i++)
-                for (int d = 0; d < 3; d++) {
-                    cwar[6 * i + d] = cwr[3 * i + d];
-                    cwar[6 * i + 3 + d] = cawr[3 * i + d];
-                }
-            if (record_tables() && h.n_cells >= 8) {
-                // cells whose weight sequences (cwa, cv, cwar over the cone) repeat bit for bit (the
-                // cells of a structured block) share one copy
-                auto seq_hash = [&](size_t c) {
-                    const size_t b = (size_t)h.cone_ptr[c], n = (size_t)h.cone_ptr[c + 1] - b;
-                    uint64_t hh = abl::hash_bits(&cwa[6 * b], 6 * n);
-                    hh = abl::hash_bits(&cv[3 * b], 3 * n, hh);
-                    return abl::hash_bits(&cwar[6 * b], 6 * n, hh);
-                };
-                auto seq_same = [&](size_t a, size_t c) {
-                    const size_t ba = (size_t)h.cone_ptr[a], na = (size_t)h.cone_ptr[a + 1] - ba;
-                    const size_t bc = (size_t)h.cone_ptr[c], nn = (size_t)h.cone_ptr[c + 1] - bc;
-                    return na == nn && std::memcmp(&cwa[6 * ba], &cwa[6 * bc], 6 * nn * sizeof(double)) == 0 &&
-                           std::memcmp(&cv[3 * ba], &cv[3 * bc], 3 * nn * sizeof(double)) == 0 &&
-                           std::memcmp(&cwar[6 * ba], &cwar[6 * bc], 6 * nn * sizeof(double)) == 0;
-                };
-                std::vector<int32_t> cls;
-                std::vector<size_t> rep;
-                const size_t ncl = abl::distinct_classes((size_t)h.n_cells, std::min(abl::kMaxRecordClasses, (size_t)h.n_cells / 8),
-                                                         seq_hash, seq_same, cls, rep);
-                if (ncl) {
-                    std::vector<int32_t> start(ncl + 1, 0), base(h.n_cells);
-                    for (size_t j = 0; j < ncl; j++) start[j + 1] = start[j] + h.cone_ptr[rep[j] + 1] - h.cone_ptr[rep[j]];
-                    std::vector<double> tw(6 * (size_t)start[ncl]), tv(3 * (size_t)start[ncl]), twr(6 * (size_t)start[ncl]);
-                    for (size_t j = 0; j < ncl; j++) {
-                        const size_t b = (size_t)h.cone_ptr[rep[j]], n = (size_t)(start[j + 1] - start[j]), o = (size_t)start[j];
-                        std::copy_n(&cwa[6 * b], 6 * n, &tw[6 * o]);
-                        std::copy_n(&cv[3 * b], 3 * n, &tv[3 * o]);
-                        std::copy_n(&cwar[6 * b], 6 * n, &twr[6 * o]);
-                    }
-                    for (int c = 0; c < h.n_cells; c++) base[c] = start[cls[c]];
-                    cwa.swap(tw);
-                    cv.swap(tv);
-                    cwar.swap(twr);
-                    fv->cone_cls.upload(base.data(), base.size());
-                    fv->n_cone_classes = (int)ncl;
-                }
+            // cone-major weights and offsets, one copy per distinct cell sequence where they repeat
+            ConeRecords cr = cone_records(h, lsq, dif, record_tables());
+            const std::vector<double>& cwa = cr.cwa;
+            const std::vector<double>& cv = cr.cv;
+            const std::vector<double>& cwar = cr.cwar;
+            const int maxc = cr.max_cone;
+            if (cr.classes) {
+                fv->cone_cls.upload(cr.base.data(), cr.base.size());
+                fv->n_cone_classes = (int)cr.classes;
             }
             fv->cwa.upload(cwa.data(), cwa.size());
             fv->cv.upload(cv.data(), cv.size());

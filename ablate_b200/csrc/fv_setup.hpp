@@ -529,4 +529,109 @@ inline uint64_t hash_bits(const double* p, size_t n, uint64_t h = 14695981039346
 // Record tables are used when the distinct records are at most this many and at most 1/8 of the items.
 constexpr size_t kMaxRecordClasses = 4096;
 
+// Per cone entry (cell-major, the cone in its canonical order): the LSQ state weight (0 across a
+// boundary face and without a state gradient) and the aux weight packed in one 6-double record (cwa),
+// the neighbour offset x_n - x_c (cv), and the neighbour's two weights for the same face packed like
+// cwa (cwar: the transposed operators of the adjoint gather). With tables, cells whose sequences (cwa,
+// cv, cwar over the cone) are equal bit for bit share one copy: the arrays then hold one sequence per
+// class and base[c] is the first entry of cell c's copy.
+struct ConeRecords {
+    std::vector<double> cwa, cv, cwar;
+    std::vector<int32_t> base;  // empty: one record per cone entry
+    size_t classes = 0;
+    int max_cone = 0;
+};
+
+inline ConeRecords cone_records(const HostMesh& h, bool lsq, bool dif, bool tables) {
+    ConeRecords r;
+    const size_t ncone = h.cone_face.size();
+    r.cwa.assign(6 * ncone, 0.0);
+    r.cv.assign(3 * ncone, 0.0);
+    r.cwar.assign(6 * ncone, 0.0);
+    for (int c = 0; c < h.n_cells; c++) {
+        r.max_cone = std::max(r.max_cone, h.cone_ptr[c + 1] - h.cone_ptr[c]);
+        for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+            const size_t f = (size_t)h.cone_face[i], sc = h.cone_side[i], q = (size_t)i;
+            for (int d = 0; d < 3; d++) {
+                if (lsq && !h.face_boundary[f]) {
+                    r.cwa[6 * q + d] = h.cgrad[6 * f + 3 * sc + d];
+                    r.cwar[6 * q + d] = h.cgrad[6 * f + 3 * (1 - sc) + d];
+                }
+                if (dif) {
+                    r.cwa[6 * q + 3 + d] = h.fgrad[6 * f + 3 * sc + d];
+                    r.cwar[6 * q + 3 + d] = h.fgrad[6 * f + 3 * (1 - sc) + d];
+                }
+                r.cv[3 * q + d] = h.fdx[6 * f + 3 * sc + d] - h.fdx[6 * f + 3 * (1 - sc) + d];
+            }
+        }
+    }
+    if (!tables || h.n_cells < 8) return r;
+    auto span = [&](size_t c) { return std::make_pair((size_t)h.cone_ptr[c], (size_t)(h.cone_ptr[c + 1] - h.cone_ptr[c])); };
+    auto seq_hash = [&](size_t c) {
+        const auto [b, n] = span(c);
+        uint64_t hh = hash_bits(&r.cwa[6 * b], 6 * n);
+        hh = hash_bits(&r.cv[3 * b], 3 * n, hh);
+        return hash_bits(&r.cwar[6 * b], 6 * n, hh);
+    };
+    auto seq_same = [&](size_t a, size_t c) {
+        const auto [ba, na] = span(a);
+        const auto [bc, nn] = span(c);
+        return na == nn && std::memcmp(&r.cwa[6 * ba], &r.cwa[6 * bc], 6 * nn * sizeof(double)) == 0 &&
+               std::memcmp(&r.cv[3 * ba], &r.cv[3 * bc], 3 * nn * sizeof(double)) == 0 &&
+               std::memcmp(&r.cwar[6 * ba], &r.cwar[6 * bc], 6 * nn * sizeof(double)) == 0;
+    };
+    std::vector<int32_t> cls;
+    std::vector<size_t> rep;
+    const size_t ncl = distinct_classes((size_t)h.n_cells, std::min(kMaxRecordClasses, (size_t)h.n_cells / 8), seq_hash, seq_same, cls, rep);
+    if (!ncl) return r;
+    std::vector<int32_t> start(ncl + 1, 0);
+    for (size_t j = 0; j < ncl; j++) start[j + 1] = start[j] + (int32_t)span(rep[j]).second;
+    const size_t nt = (size_t)start[ncl];
+    std::vector<double> tw(6 * nt), tv(3 * nt), twr(6 * nt);
+    for (size_t j = 0; j < ncl; j++) {
+        const auto [b, n] = span(rep[j]);
+        const size_t o = (size_t)start[j];
+        std::copy_n(&r.cwa[6 * b], 6 * n, &tw[6 * o]);
+        std::copy_n(&r.cv[3 * b], 3 * n, &tv[3 * o]);
+        std::copy_n(&r.cwar[6 * b], 6 * n, &twr[6 * o]);
+    }
+    r.base.resize(h.n_cells);
+    for (int c = 0; c < h.n_cells; c++) r.base[c] = start[cls[c]];
+    r.cwa.swap(tw);
+    r.cv.swap(tv);
+    r.cwar.swap(twr);
+    r.classes = ncl;
+    return r;
+}
+
+// Per tile face record one 10-double geometry record: area normal (3), the face centroid minus each
+// side's centroid (6), a pad. With tables, records equal bit for bit are stored once and cls[i] gives
+// record i's copy.
+struct GeoRecords {
+    std::vector<double> geo;
+    std::vector<uint16_t> cls;  // empty: one record per tile face record
+};
+
+inline GeoRecords tile_geometry(const Tiles& tl, bool tables) {
+    GeoRecords g;
+    const size_t ntf = tl.tf_cells.size() / 2;
+    g.geo.assign(10 * ntf, 0.0);
+    for (size_t i = 0; i < ntf; i++) {
+        for (int d = 0; d < 3; d++) g.geo[10 * i + d] = tl.tf_normal[3 * i + d];
+        for (int z = 0; z < 6; z++) g.geo[10 * i + 3 + z] = tl.tf_fdx[6 * i + z];
+    }
+    if (!tables || ntf < 8) return g;
+    std::vector<int32_t> cls;
+    std::vector<size_t> rep;
+    const size_t ng = distinct_classes(
+        ntf, std::min(kMaxRecordClasses, ntf / 8), [&](size_t k) { return hash_bits(&g.geo[10 * k], 10); },
+        [&](size_t a, size_t b) { return std::memcmp(&g.geo[10 * a], &g.geo[10 * b], 10 * sizeof(double)) == 0; }, cls, rep);
+    if (!ng) return g;
+    std::vector<double> table(10 * ng);
+    for (size_t j = 0; j < ng; j++) std::copy_n(&g.geo[10 * rep[j]], 10, &table[10 * j]);
+    g.geo.swap(table);
+    g.cls.assign(cls.begin(), cls.end());
+    return g;
+}
+
 }  // namespace abl
