@@ -75,6 +75,13 @@ void validate_physics(const abl_physics_desc* p) {
     if (p->reconstruction != ABL_RECON_UPWIND && p->reconstruction != ABL_RECON_LEASTSQUARES) throw std::invalid_argument("unknown reconstruction");
     if (p->limiter < ABL_LIMITER_NONE || p->limiter > ABL_LIMITER_SIN) throw std::invalid_argument("unknown limiter");
     if (p->transport < ABL_TRANSPORT_NONE || p->transport > ABL_TRANSPORT_CONSTANT_LEWIS) throw std::invalid_argument("unknown transport model");
+    if (p->species_diff) {
+        // SpeciesTransport::Setup: the diffusion property size must be 1 or the number of species
+        if (p->transport != ABL_TRANSPORT_CONSTANT || p->n_species <= 0)
+            throw std::invalid_argument("per-species diffusivities need the constant transport model and species");
+        for (int k = 0; k < p->n_species; k++)
+            if (!std::isfinite(p->species_diff[k])) throw std::invalid_argument("per-species diffusivity must be finite");
+    }
 }
 
 Phys make_phys(const abl_physics_desc* p) {
@@ -362,6 +369,10 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         // the mixture EOS keeps T resident (secant guess + face temperatures); a perfect gas recomputes it
         fv->need_aux = physics->eos == ABL_EOS_NASA7;
         upload_species(physics, fv->phys, fv->nasa7, fv->mw, fv->inv_mw, fv->href);
+        if (physics->species_diff && physics->species_diffusion) {
+            fv->diff_k.upload(physics->species_diff, physics->n_species);
+            fv->phys.diff_k = fv->diff_k.p;
+        }
 
         fv->face_cells.upload(reinterpret_cast<const int2*>(h.face_cells.data()), h.n_faces);
         fv->kind.upload(h.kind.data(), h.kind.size());

@@ -609,15 +609,17 @@ __device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* norma
 #pragma unroll
             for (int s = 0; s < NS; ++s) {
                 const double hs = P.eos == ABL_EOS_NASA7 ? nasa_h_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s] - P.href[s] : 0.0;
+                // one constant D_k per species (no state dependence), or the transport model's D
+                const double Ds = P.diff_k ? P.diff_k[s] : diff;
                 double hsb = 0;
 #pragma unroll
                 for (int d = 0; d < DIM; ++d) {
                     const double gy = gf[yoff + s * DIM + d];
                     const double q = -normal[d] * (fb[D::NE + s] + hs * fb[1]);
-                    rhob += q * diff * gy;
-                    Db += q * density * gy;
-                    gfb[yoff + s * DIM + d] += q * density * diff;
-                    hsb -= normal[d] * density * diff * gy * fb[1];
+                    rhob += q * Ds * gy;
+                    if (!P.diff_k) Db += q * density * gy;
+                    gfb[yoff + s * DIM + d] += q * density * Ds;
+                    hsb -= normal[d] * density * Ds * gy * fb[1];
                 }
                 if (P.eos == ABL_EOS_NASA7) Tb += hsb * nasa_cp_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s];
             }

@@ -78,7 +78,7 @@ struct abl_fv {
     abl::DevBuf<uint8_t> kind;
     abl::DevBuf<int> cone_ptr;
     abl::DevBuf<double> fdx, ivol, cgrad, fgrad;
-    abl::DevBuf<double> nasa7, mw, inv_mw, href;
+    abl::DevBuf<double> nasa7, mw, inv_mw, href, diff_k;
     // tiles
     abl::DevBuf<int> tile_cell_ptr, tile_cells, tile_face_ptr, tc_fptr;
     abl::DevBuf<int2> tf_cells;

@@ -704,7 +704,8 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
         }
         if constexpr (NS > 0) {
             if (spdif) {
-                // SpeciesTransport::DiffusionEnergyFlux + DiffusionSpeciesFlux (speciesTransport.cpp:112-228)
+                // SpeciesTransport::DiffusionEnergyFlux + DiffusionSpeciesFlux (speciesTransport.cpp:112-228),
+                // or their VariableDiffusionCoefficient forms with one constant D_k per species (:154-194, :230-261)
                 const S density = fs[0];
                 S hs[NS];
                 if (P.eos == ABL_EOS_NASA7) {
@@ -719,11 +720,12 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 #pragma unroll
                 for (int s = 0; s < NS; ++s) {
                     S sf = 0;
+                    const S Ds = P.diff_k ? S(P.diff_k[s]) : diff;
 #pragma unroll
                     for (int d = 0; d < DIM; ++d) {
                         const S gy = to_state<S>(G(0.5) * gL[yoff + s * DIM + d] + G(0.5) * gR[yoff + s * DIM + d]);
-                        ef += -normal[d] * density * diff * hs[s] * gy;
-                        sf += -normal[d] * density * diff * gy;
+                        ef += -normal[d] * density * Ds * hs[s] * gy;
+                        sf += -normal[d] * density * Ds * gy;
                     }
                     flux[D::NE + s] += sf;
                 }

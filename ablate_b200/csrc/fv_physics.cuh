@@ -77,6 +77,7 @@ struct Phys {
     const double* mw;     // [ns]
     const double* inv_mw; // [ns]
     const double* href;   // [ns] reference enthalpy at 298.15 K, J/kg
+    const double* diff_k; // [ns] per-species constant diffusivities (Constant model with one per species), or null
 };
 
 constexpr double kRuniv = 8314.46261815324;  // J/(kmol K)

@@ -189,12 +189,23 @@ class PressureGradientScaling:
 # transport
 # ---------------------------------------------------------------------------------------------
 class Constant:
-    def __init__(self, k: float = 0.0, mu: float = 0.0, diff: float = 0.0):
-        self.k, self.mu, self.diff = float(k), float(mu), float(diff)
+    """src/eos/transport/constant.cpp: constant k, mu and diffusivity; the diffusivity is one value, or
+    one per species (then SpeciesTransport registers its VariableDiffusionCoefficient fluxes)."""
+
+    def __init__(self, k: float = 0.0, mu: float = 0.0, diff=0.0):
+        self.k, self.mu = float(k), float(mu)
+        if np.ndim(diff) == 0:
+            self.diff, self.species_diff = float(diff), None
+        else:
+            self.diff, self.species_diff = 0.0, np.ascontiguousarray(diff, dtype=np.float64)
 
     def _fill(self, p):
         p.transport = L.TRANSPORT_CONSTANT
         p.k, p.mu, p.diff = self.k, self.mu, self.diff
+        if self.species_diff is not None:
+            if len(self.species_diff) != p.n_species:
+                raise ValueError("The diffusion property size must be 1 or number of species")
+            p.species_diff = L.dptr(self.species_diff)
 
 
 class Sutherland:

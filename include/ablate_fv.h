@@ -152,6 +152,11 @@ typedef struct abl_physics_desc {
     int32_t diffusion;          /* NavierStokesTransport::DiffusionFlux registered */
     int32_t species_advection;  /* SpeciesTransport::AdvectionFlux registered */
     int32_t species_diffusion;  /* SpeciesTransport::DiffusionSpeciesFlux + DiffusionEnergyFlux registered */
+    const double* species_diff; /* [n_species] per-species diffusivities D_k of the Constant model given one
+                                   value per species, which registers DiffusionSpeciesFluxVariableDiffusionCoefficient
+                                   and DiffusionEnergyFluxVariableDiffusionCoefficient instead
+                                   (src/finiteVolume/processes/speciesTransport.cpp:64-75, 154-194, 230-261);
+                                   ABL_TRANSPORT_CONSTANT only. NULL: the scalar diff */
 } abl_physics_desc;
 
 typedef struct abl_fv abl_fv; /* opaque handle: one mesh + physics resident on one device */

@@ -960,7 +960,8 @@ struct Rhs {
         flux[0] = 0.0;
     }
 
-    // SpeciesTransport::DiffusionEnergyFlux (speciesTransport.cpp:112-152): rhoE contribution only
+    // SpeciesTransport::DiffusionEnergyFlux (speciesTransport.cpp:112-152): rhoE contribution only; with
+    // one diffusivity per species, DiffusionEnergyFluxVariableDiffusionCoefficient (:154-194)
     double species_diffusion_energy(const double* normal, const double* field, const double* aux, const double* gradAux) const {
         const double density = field[0];
         const double temperature = aux[0];
@@ -969,18 +970,22 @@ struct Rhs {
         double diff = tr.diff(field, temperature);
         double e = 0.0;
         const int yoff = (1 + dim) * dim;  // aux gradient offset of the Yi block
-        for (int sp = 0; sp < ns; ++sp)
-            for (int d = 0; d < dim; ++d) e += -normal[d] * density * diff * hs[sp] * gradAux[yoff + sp * dim + d];
+        for (int sp = 0; sp < ns; ++sp) {
+            const double dsp = p->species_diff ? p->species_diff[sp] : diff;
+            for (int d = 0; d < dim; ++d) e += -normal[d] * density * dsp * hs[sp] * gradAux[yoff + sp * dim + d];
+        }
         return e;
     }
-    // SpeciesTransport::DiffusionSpeciesFlux (speciesTransport.cpp:196-228)
+    // SpeciesTransport::DiffusionSpeciesFlux (speciesTransport.cpp:196-228); with one diffusivity per
+    // species, DiffusionSpeciesFluxVariableDiffusionCoefficient (:230-261)
     void species_diffusion(const double* normal, const double* field, const double* aux, const double* gradAux, double* flux) const {
         const double density = field[0];
         double diff = tr.diff(field, aux[0]);
         const int yoff = (1 + dim) * dim;
         for (int sp = 0; sp < ns; ++sp) {
+            const double dsp = p->species_diff ? p->species_diff[sp] : diff;
             flux[sp] = 0;
-            for (int d = 0; d < dim; ++d) flux[sp] += -normal[d] * density * diff * gradAux[yoff + sp * dim + d];
+            for (int d = 0; d < dim; ++d) flux[sp] += -normal[d] * density * dsp * gradAux[yoff + sp * dim + d];
         }
     }
 

@@ -69,7 +69,11 @@ def case(name: str) -> Workload:
         eos = synthetic_mixture(ns, 7)
         U = _perturbed_state(mesh, rng, 3, ns, eos)
         flux = fv.AusmpUp(0.3)
-        tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
+        if name.endswith("_dk"):
+            # the Constant model with one diffusivity per species (the VariableDiffusionCoefficient fluxes)
+            tr = fv.Constant(k=0.03, mu=2e-5, diff=np.linspace(2e-5, 1.2e-4, ns))
+        else:
+            tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
         procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
         return Workload(name, mesh, eos, procs, "leastsquares", "vanleer", U, name)
     if name.startswith("pgspecies3d_"):
@@ -108,6 +112,7 @@ CASES = [
     "box2d_ausm_none_none",
     "species3d_ns5",
     "species3d_ns9",
+    "species3d_ns5_dk",
     "pgspecies3d_ns2",
     "tets3d_ns9",
     "tets3d_pg_minmod",
