@@ -710,20 +710,44 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
         }
 #pragma unroll
         for (int k = 0; k < D::NC; k++) fs[k] = c[k] * 0.5 + xch(mask, c[k]) * 0.5;
+        // the face gradient: in 1D the two-cell LeastSquares stencil's (w_L a_L + w_R a_R, the same sum
+        // in both lanes), else the average of the two cells' aux gradients
+        double wme = 0.0;
+        if constexpr (DIM == 1) {
+            const double xme = fdxo[0], xot = xch(mask, fdxo[0]);  // each lane holds its side's offset
+            const double fdx2[6] = {side ? xot : xme, 0.0, 0.0, side ? xme : xot, 0.0, 0.0};
+            double wl, wr;
+            face_weights_1d(fdx2, &wl, &wr);
+            wme = side ? wr : wl;
+            const double wot = side ? wl : wr;
+            double a[D::NA];
+            cell_aux<DIM, NS>(P, c, aux, me, a);
 #pragma unroll
-        for (int k = 0; k < D::NA * DIM; k++) {
-            const double gm = __ldg(agrad + (size_t)me * GR::AS + k);
-            gf[k] = 0.5 * gm + 0.5 * xch(mask, gm);
+            for (int k = 0; k < D::NA; k++) {
+                const double mine = a[k] * wme, other = xch(mask, a[k]) * wot;
+                gf[k] = side ? other + mine : mine + other;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < D::NA * DIM; k++) {
+                const double gm = __ldg(agrad + (size_t)me * GR::AS + k);
+                gf[k] = 0.5 * gm + 0.5 * xch(mask, gm);
+            }
         }
         double fsb[D::NC], fab[D::NA], gfb[D::NA * DIM];
         diffusion_vjp<DIM, NS>(P, normal, fs, fa, gf, dif, spdif, fb, fsb, fab, gfb);
         if (dst) {
 #pragma unroll
             for (int k = 0; k < D::NC; k++) dst[AR::U + k] += 0.5 * fsb[k];
+            if constexpr (DIM == 1) {
 #pragma unroll
-            for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k];
+                for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k] + wme * gfb[k];
+            } else {
 #pragma unroll
-            for (int k = 0; k < D::NA * DIM; k++) dst[AR::GA + k] += 0.5 * gfb[k];
+                for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k];
+#pragma unroll
+                for (int k = 0; k < D::NA * DIM; k++) dst[AR::GA + k] += 0.5 * gfb[k];
+            }
         }
     }
 }

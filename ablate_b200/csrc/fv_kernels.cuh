@@ -526,6 +526,19 @@ __device__ __forceinline__ void advection_split(const Phys& P, const double* nor
     }
 }
 
+// 1D face-gradient weights of the two cells of a face: the FaceInterpolant's 1D stencil::LeastSquares
+// (faceInterpolant.cpp:32-36, stencils/leastSquares.cpp:5-122). With x_i the offset of cell i's centroid
+// from the face centroid, the least-squares weights x_i / (x_L^2 + x_R^2), less their mean (the value
+// weights are 1/2 each). fdx holds the face centroid minus each side's centroid.
+__host__ __device__ __forceinline__ void face_weights_1d(const double* fdx, double* wl, double* wr) {
+    const double xl = -fdx[0], xr = -fdx[3];
+    const double s = xl * xl + xr * xr;
+    const double gl = xl / s, gr = xr / s;
+    const double m = 0.5 * gl + 0.5 * gr;
+    *wl = gl - m;
+    *wr = gr - m;
+}
+
 // ---------------------------------------------------------------------------------------------------
 // flux of one face: advection (NS + species) and diffusion (NS + species), summed per component
 template <int DIM, int NS, class G, int FK>
@@ -664,8 +677,17 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 #pragma unroll
         for (int k = 0; k < D::NA; k++) fa[k] = aL[k] * 0.5 + aR[k] * 0.5;
         G gL[D::NA * DIM], gR[D::NA * DIM];
-        load_row<D::NA * DIM, G>(agrad + (size_t)L * GR::AS, gL);
-        load_row<D::NA * DIM, G>(agrad + (size_t)R * GR::AS, gR);
+        if constexpr (DIM == 1) {
+            // in 1D the face gradient is the two-cell LeastSquares stencil's; both sides carry it, so
+            // the averages below return it exactly
+            double wl, wr;
+            face_weights_1d(fdx, &wl, &wr);
+#pragma unroll
+            for (int k = 0; k < D::NA; k++) gL[k] = gR[k] = static_cast<G>(aL[k] * wl + aR[k] * wr);
+        } else {
+            load_row<D::NA * DIM, G>(agrad + (size_t)L * GR::AS, gL);
+            load_row<D::NA * DIM, G>(agrad + (size_t)R * GR::AS, gR);
+        }
         S mu, kc, diff;
         transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
         if (dif) {

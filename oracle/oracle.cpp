@@ -782,8 +782,35 @@ void cell_stencil(const abl_mesh_desc* m, const Topo& t, int cell, Stencil& s) {
             for (int d = 0; d < dim; d++) s.gw[fn * dim + d] -= org[gn * dim + d] * s.weights[fn];
 }
 
+// stencil::LeastSquares of one face, the 1D choice of the FaceInterpolant (faceInterpolant.cpp:32-36,
+// src/finiteVolume/stencils/leastSquares.cpp:5-122): the cells sharing the face's node (in 1D its two
+// support cells), value weights 1/2, gradient weights the least-squares operator of the offsets
+// x_cell - x_face less its value-weighted sum
+void face_stencil_1d(const abl_mesh_desc* m, int f, Stencil& out) {
+    const int a = m->face_cells[2 * f], b = m->face_cells[2 * f + 1];
+    out.cells = {std::min(a, b), std::max(a, b)};
+    out.weights = {0.5, 0.5};
+    // offsets to the face centroid, periodic image resolved: the face centroid is given in the left
+    // cell's frame and the right cell is seen from there at its centroid + face_shift
+    const double sh = m->face_shift ? m->face_shift[3 * (size_t)f] : 0.0;
+    std::vector<double> dx(2);
+    for (int i = 0; i < 2; i++) {
+        const int c = out.cells[i];
+        dx[i] = m->cell_centroid[3 * (size_t)c] + (c == b ? sh : 0.0) - m->face_centroid[3 * (size_t)f];
+    }
+    out.gw.assign(2, 0.0);
+    pinv_rows(2, 1, dx.data(), out.gw.data());
+    const std::vector<double> org = out.gw;
+    for (int gn = 0; gn < 2; gn++)
+        for (int fn = 0; fn < 2; fn++) out.gw[fn] -= org[gn] * out.weights[fn];
+}
+
 void face_stencil(const abl_mesh_desc* m, const Topo& t, int f, Stencil& out) {
     const int dim = m->dim;
+    if (dim == 1) {
+        face_stencil_1d(m, f, out);
+        return;
+    }
     Stencil L, R;
     cell_stencil(m, t, m->face_cells[2 * f], L);
     cell_stencil(m, t, m->face_cells[2 * f + 1], R);

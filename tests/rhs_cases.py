@@ -54,6 +54,14 @@ def case(name: str) -> Workload:
         U[mesh.cell_kind == L.CELL_BOUNDARY] *= 1.0 + 0.01 * rng.standard_normal((int((mesh.cell_kind == L.CELL_BOUNDARY).sum()), 4))
         return Workload(name, mesh, eos, [fv.NavierStokesTransport({}, eos, fc, trm)], "leastsquares" if lim != "upwind" else "upwind",
                         lim if lim != "upwind" else "none", U, name)
+    if name.startswith("box1d_visc"):
+        # 1D Navier-Stokes with conduction and viscosity, LSQ + minmod: the 1D face stencil
+        periodic = name.endswith("_periodic")
+        mesh = box_mesh((32,), periodic=(periodic,))
+        eos = fv.PerfectGas({"gamma": 1.4, "Rgas": 287.0})
+        U = _perturbed_state(mesh, rng, 1)
+        procs = [fv.NavierStokesTransport({}, eos, fv.AusmpUp(0.3), fv.Constant(k=0.6, mu=2e-3))]
+        return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
     if name == "box1d_riemann_upwind":
         mesh = box_mesh((40,))
         eos = fv.PerfectGas({"gamma": 1.4, "Rgas": 287.0})
@@ -102,6 +110,8 @@ CASES = [
     "sod2d_natural_order",
     "tgv3d_natural_order",
     "box1d_riemann_upwind",
+    "box1d_visc",
+    "box1d_visc_periodic",
     "tgv3d_ausmpup_lsq_minmod_visc",
     "box2d_ausm_upwind_none",
     "box2d_ausm_minmod_const",
