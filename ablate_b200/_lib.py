@@ -66,7 +66,7 @@ class PhysicsDesc(C.Structure):
         ("reconstruction", C.c_int32), ("limiter", C.c_int32), ("max_lim_grad", C.c_double),
         ("transport", C.c_int32), ("k", C.c_double), ("mu", C.c_double), ("diff", C.c_double),
         ("advection", C.c_int32), ("diffusion", C.c_int32), ("species_advection", C.c_int32), ("species_diffusion", C.c_int32),
-        ("species_diff", _dp),
+        ("species_diff", _dp), ("species_advection_compact", C.c_int32),
     ]
 
 

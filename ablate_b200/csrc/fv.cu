@@ -96,6 +96,7 @@ Phys make_phys(const abl_physics_desc* p) {
     P.diffusion = p->diffusion;
     P.sp_adv = p->species_advection;
     P.sp_dif = p->species_diffusion;
+    P.sp_compact = p->species_advection_compact;
     P.gamma = p->gamma;
     P.r_gas = p->r_gas;
     P.minf = p->ausmpup_minf;

@@ -514,7 +514,18 @@ __device__ __forceinline__ void advection_vjp_side(const Phys& P, unsigned mask,
             for (int n = 0; n < DIM; n++) velb[n] += Hb * vel[n] + 0.5 * mA * fb[2 + n];
         }
     }
-    if (NS > 0 && spadv) {
+    if (NS > 0 && spadv && dir == ABL_DIR_NA && P.sp_compact) {
+        // compact process, no direction: flux_s = mA (rhoY_L + rhoY_R) / (rho_L + rho_R) (both halves)
+        const double rhoM = 0.5 * (rho + rho_o), irm = 1.0 / rhoM;
+#pragma unroll
+        for (int s = 0; s < NS; s++) {
+            const double ry = u[D::NE + s], ry_o = xch(mask, ry);
+            const double num = 0.5 * (side ? ry + ry_o : ry_o + ry);
+            mfb += areaMag * num * irm * fb[D::NE + s];
+            ub[D::NE + s] += 0.5 * mA * irm * fb[D::NE + s];
+            ub[0] -= 0.5 * mA * num * irm * irm * fb[D::NE + s];
+        }
+    } else if (NS > 0 && spadv) {
 #pragma unroll
         for (int s = 0; s < NS; s++) {
             const double Y = u[D::NE + s] * irho;

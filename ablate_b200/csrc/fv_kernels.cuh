@@ -653,10 +653,15 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
                 }
             }
             if (spadv) {
-                // SpeciesTransport::AdvectionFlux (speciesTransport.cpp:263-341): LEFT upwinds, anything else takes the right state
+                // SpeciesTransport::AdvectionFlux (speciesTransport.cpp:263-341): LEFT upwinds, anything else takes the right
+                // state; the compact process averages where there is no direction (compactCompressibleNSSpeciesTransport.cpp:257-259)
                 if (dir == ABL_DIR_LEFT) {
 #pragma unroll
                     for (int s = 0; s < NS; s++) flux[D::NE + s] = (mf * uL[D::NE + s] * irhoL) * areaMag;
+                } else if (dir == ABL_DIR_NA && P.sp_compact) {
+                    const S rhoM = 0.5 * (uL[0] + uR[0]);
+#pragma unroll
+                    for (int s = 0; s < NS; s++) flux[D::NE + s] = mf * 0.5 * (uR[D::NE + s] + uL[D::NE + s]) / rhoM * areaMag;
                 } else {
 #pragma unroll
                     for (int s = 0; s < NS; s++) flux[D::NE + s] = (mf * uR[D::NE + s] * irhoR) * areaMag;

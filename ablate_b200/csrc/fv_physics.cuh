@@ -70,6 +70,7 @@ ABL_HD bool dfinite(double x) { return isfinite(x); }
 struct Phys {
     int32_t eos, ns, flux, recon, limiter, transport;
     int32_t advection, diffusion, sp_adv, sp_dif;
+    int32_t sp_compact;  // species advection of the compact NS + species process (NA direction averages)
     int32_t jvp_frozen_limiter;  // tangent evaluations hold the limiter factor at its value (dphi = 0)
     double gamma, r_gas, minf, alpha, max_lim_grad;
     double k, mu, diff;

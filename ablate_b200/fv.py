@@ -259,6 +259,23 @@ class SpeciesTransport:
             flow.RegisterRHSFunction("SpeciesTransport::DiffusionSpeciesFlux", self.transport)
 
 
+class CompactCompressibleNSSpeciesTransport:
+    """src/finiteVolume/processes/compactCompressibleNSSpeciesTransport.cpp:12-160: Navier-Stokes and
+    species transport in one process. Its fluxes are NavierStokesTransport's and SpeciesTransport's,
+    except the species advection where the flux calculator gives no direction (the average flux):
+    there rho Y_k is carried as (rho Y_L + rho Y_R) / (rho_L + rho_R)."""
+
+    def __init__(self, parameters: dict | None, eos, fluxCalculator=None, transport=None, pgs=None):
+        self.parameters = parameters or {}
+        self.eos, self.fluxCalculator, self.transport = eos, fluxCalculator, transport
+
+    def Setup(self, flow: "FiniteVolumeSolver"):
+        if self.fluxCalculator is not None:
+            flow.RegisterRHSFunction("CompactCompressibleNSSpeciesTransport::AdvectionFlux", self.fluxCalculator)
+        if self.transport is not None:
+            flow.RegisterRHSFunction("CompactCompressibleNSSpeciesTransport::DiffusionFlux", self.transport)
+
+
 # ---------------------------------------------------------------------------------------------
 # solver
 # ---------------------------------------------------------------------------------------------
@@ -296,6 +313,19 @@ def make_physics(eos, processes, petscfv_type: str = "upwind", limiter: str = "n
                 flux = proc.fluxCalculator
             if proc.transport is not None:
                 p.species_diffusion = 1
+                proc.transport._fill(p)
+        elif isinstance(proc, CompactCompressibleNSSpeciesTransport):
+            species = bool(eos.GetSpeciesVariables())
+            if proc.fluxCalculator is not None:
+                if flux is not None and type(flux) is not type(proc.fluxCalculator):
+                    raise ValueError("processes must share one flux calculator type")
+                flux = proc.fluxCalculator
+                p.advection = 1
+                p.species_advection = int(species)
+                p.species_advection_compact = int(species)
+            if proc.transport is not None:
+                p.diffusion = 1
+                p.species_diffusion = int(species)
                 proc.transport._fill(p)
     if flux is not None:
         p.flux = flux.kind

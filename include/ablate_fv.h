@@ -157,6 +157,10 @@ typedef struct abl_physics_desc {
                                    and DiffusionEnergyFluxVariableDiffusionCoefficient instead
                                    (src/finiteVolume/processes/speciesTransport.cpp:64-75, 154-194, 230-261);
                                    ABL_TRANSPORT_CONSTANT only. NULL: the scalar diff */
+    int32_t species_advection_compact; /* the species advection of CompactCompressibleNSSpeciesTransport::AdvectionFlux
+                                          (compactCompressibleNSSpeciesTransport.cpp:162-271): where the flux calculator
+                                          gives no direction (NA), rho Y_k is carried as
+                                          (rho Y_L + rho Y_R) / (rho_L + rho_R) instead of the right state */
 } abl_physics_desc;
 
 typedef struct abl_fv abl_fv; /* opaque handle: one mesh + physics resident on one device */

@@ -957,8 +957,13 @@ struct Rhs {
         eos.property_T(ABL_PROP_SPEED_OF_SOUND, fieldR, temperatureR, &aR);
         eos.property_T(ABL_PROP_PRESSURE, fieldR, temperatureR, &pR);
         double massFlux;
-        if (flux_calc(fc, normalVelocityL, aL, densityL, pL, normalVelocityR, aR, densityR, pR, &massFlux, nullptr) == ABL_DIR_LEFT) {
+        const int dir = flux_calc(fc, normalVelocityL, aL, densityL, pL, normalVelocityR, aR, densityR, pR, &massFlux, nullptr);
+        if (dir == ABL_DIR_LEFT) {
             for (int sp = 0; sp < ns; sp++) flux[sp] = (massFlux * fieldL[neuler + sp] / densityL) * areaMag;
+        } else if (dir == ABL_DIR_NA && p->species_advection_compact) {
+            // CompactCompressibleNSSpeciesTransport::AdvectionFlux (compactCompressibleNSSpeciesTransport.cpp:257-259)
+            for (int sp = 0; sp < ns; sp++)
+                flux[sp] = massFlux * 0.5 * (fieldR[neuler + sp] + fieldL[neuler + sp]) / (0.5 * (densityL + densityR)) * areaMag;
         } else {
             for (int sp = 0; sp < ns; sp++) flux[sp] = (massFlux * fieldR[neuler + sp] / densityR) * areaMag;
         }
@@ -1294,6 +1299,22 @@ int orc_ns_advection_flux(const abl_physics_desc* physics, int dim, const double
         double nrm[3] = {0, 0, 0};
         for (int d = 0; d < dim; d++) nrm[d] = normal[d];
         r.ns_advection(nrm, fieldL, fieldR, TL, TR, flux);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return ABL_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int orc_species_advection_flux(const abl_physics_desc* physics, int dim, const double* normal, const double* fieldL, const double* fieldR,
+                                double TL, double TR, double* flux) {
+    try {
+        abl_mesh_desc m{};
+        m.dim = dim;
+        Rhs r(&m, physics);
+        double nrm[3] = {0, 0, 0};
+        for (int d = 0; d < dim; d++) nrm[d] = normal[d];
+        r.species_advection(nrm, fieldL, fieldR, TL, TR, flux);
         return 0;
     } catch (const std::exception& e) {
         g_err = e.what();

@@ -36,6 +36,11 @@ int orc_stress_tensor(int dim, double mu, const double* grad_vel, double* tau);
  * area-weighted normal, fieldL/R the euler field, TL/TR the aux temperature, flux[2+dim] out. */
 int orc_ns_advection_flux(const abl_physics_desc* physics, int dim, const double* normal, const double* fieldL, const double* fieldR,
                           double TL, double TR, double* flux);
+/* SpeciesTransport::AdvectionFlux for one face (speciesTransport.cpp:263-341), or the species part of
+ * CompactCompressibleNSSpeciesTransport::AdvectionFlux when physics->species_advection_compact; fieldL/R
+ * the euler + densityYi fields, flux[n_species] out. */
+int orc_species_advection_flux(const abl_physics_desc* physics, int dim, const double* normal, const double* fieldL, const double* fieldR,
+                               double TL, double TR, double* flux);
 
 /* PetscLimiterLimit restatement for the ABL_LIMITER_* kinds */
 double orc_limiter(int kind, double f);

@@ -28,6 +28,8 @@ def _load():
     lib.orc_stress_tensor.restype = C.c_int
     lib.orc_ns_advection_flux.argtypes = [C.POINTER(L.PhysicsDesc), C.c_int, dp, dp, dp, C.c_double, C.c_double, dp]
     lib.orc_ns_advection_flux.restype = C.c_int
+    lib.orc_species_advection_flux.argtypes = [C.POINTER(L.PhysicsDesc), C.c_int, dp, dp, dp, C.c_double, C.c_double, dp]
+    lib.orc_species_advection_flux.restype = C.c_int
     lib.orc_limiter.argtypes = [C.c_int, C.c_double]
     lib.orc_limiter.restype = C.c_double
     lib.orc_lsq_face_weights.argtypes = [C.POINTER(L.MeshDesc), dp]
@@ -86,6 +88,16 @@ def ns_advection_flux(physics, dim, normal, fieldL, fieldR, TL=300.0, TR=300.0):
     b = np.ascontiguousarray(fieldR, dtype=np.float64)
     out = np.zeros(2 + dim)
     _check(lib.orc_ns_advection_flux(C.byref(physics), dim, L.dptr(n), L.dptr(a), L.dptr(b), TL, TR, L.dptr(out)), "advection flux")
+    return out
+
+
+def species_advection_flux(physics, dim, normal, fieldL, fieldR, TL=300.0, TR=300.0):
+    n = np.ascontiguousarray(normal, dtype=np.float64)
+    a = np.ascontiguousarray(fieldL, dtype=np.float64)
+    b = np.ascontiguousarray(fieldR, dtype=np.float64)
+    out = np.zeros(physics.n_species)
+    _check(lib.orc_species_advection_flux(C.byref(physics), dim, L.dptr(n), L.dptr(a), L.dptr(b), TL, TR, L.dptr(out)),
+           "species advection flux")
     return out
 
 

@@ -84,6 +84,15 @@ def case(name: str) -> Workload:
             tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
         procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
         return Workload(name, mesh, eos, procs, "leastsquares", "vanleer", U, name)
+    if name == "compact3d_avg_ns5":
+        # the compact NS + species process with the average flux (no direction: the averaged species
+        # advection), per-species diffusivities
+        mesh = box_mesh((6, 5, 4), lower=(0, 0, 0), upper=(0.6, 0.5, 0.4), periodic=(True, False, False))
+        eos = synthetic_mixture(5, 7)
+        U = _perturbed_state(mesh, rng, 3, 5, eos)
+        tr = fv.Constant(k=0.03, mu=2e-5, diff=np.linspace(3e-5, 9e-5, 5))
+        procs = [fv.CompactCompressibleNSSpeciesTransport({}, eos, fv.AverageFlux(), tr)]
+        return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
     if name.startswith("pgspecies3d_"):
         ns = int(name.split("_")[1][2:])
         mesh = box_mesh((5, 4, 4), periodic=(False, True, True))
@@ -123,6 +132,7 @@ CASES = [
     "species3d_ns5",
     "species3d_ns9",
     "species3d_ns5_dk",
+    "compact3d_avg_ns5",
     "pgspecies3d_ns2",
     "tets3d_ns9",
     "tets3d_pg_minmod",

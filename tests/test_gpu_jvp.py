@@ -24,7 +24,7 @@ from tests import rhs_cases as R
 pytestmark = pytest.mark.gpu
 
 CASES = ["tgv3d_ausmpup_lsq_minmod_visc", "box2d_ausm_upwind_none", "box2d_ausmpup_vanleer_suth", "box2d_riemann_vanalbada_none",
-         "species3d_ns5", "species3d_ns5_dk", "box1d_visc", "box1d_visc_periodic", "pgspecies3d_ns2", "sod2d_ausm_upwind", "tets3d_ns9", "tets3d_pg_minmod"]
+         "species3d_ns5", "species3d_ns5_dk", "compact3d_avg_ns5", "box1d_visc", "box1d_visc_periodic", "pgspecies3d_ns2", "sod2d_ausm_upwind", "tets3d_ns9", "tets3d_pg_minmod"]
 
 
 def _direction(w, seed):

@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 CASES = ["tgv3d_ausmpup_lsq_minmod_visc", "box2d_ausm_upwind_none", "box2d_ausm_minmod_const", "box2d_ausmpup_vanleer_suth",
          "box2d_riemann_vanalbada_none", "box2d_avg_sin_const", "box2d_off_zero_const", "box1d_riemann_upwind", "sod2d_ausm_upwind",
-         "species3d_ns5", "species3d_ns9", "species3d_ns5_dk", "box1d_visc", "box1d_visc_periodic", "pgspecies3d_ns2", "tets3d_ns9", "tets3d_pg_minmod"]
+         "species3d_ns5", "species3d_ns9", "species3d_ns5_dk", "compact3d_avg_ns5", "box1d_visc", "box1d_visc_periodic", "pgspecies3d_ns2", "tets3d_ns9", "tets3d_pg_minmod"]
 
 
 def _scale(U):
