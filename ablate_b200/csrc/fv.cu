@@ -135,6 +135,7 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
             case 100: FN<1, 0>(fv, __VA_ARGS__); break;                                                                            \
             case 200: FN<2, 0>(fv, __VA_ARGS__); break;                                                                            \
             case 202: FN<2, 2>(fv, __VA_ARGS__); break;                                                                            \
+            case 203: FN<2, 3>(fv, __VA_ARGS__); break;                                                                            \
             case 300: FN<3, 0>(fv, __VA_ARGS__); break;                                                                            \
             case 302: FN<3, 2>(fv, __VA_ARGS__); break;                                                                            \
             case 305: FN<3, 5>(fv, __VA_ARGS__); break;                                                                            \
@@ -157,7 +158,7 @@ void dispatch_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cud
 
 bool rhs_supported(int dim, int ns) {
     const int key = dim * 100 + ns;
-    return key == 100 || key == 200 || key == 202 || key == 300 || key == 302 || key == 305 || key == 309;
+    return key == 100 || key == 200 || key == 202 || key == 203 || key == 300 || key == 302 || key == 305 || key == 309;
 }
 
 // ---- batch kernels ------------------------------------------------------------------------------

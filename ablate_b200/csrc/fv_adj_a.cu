@@ -5,5 +5,6 @@ namespace abl {
 template void run_vjp<1, 0>(abl_fv*, const double*, const double*, double*, cudaStream_t);
 template void run_vjp<2, 0>(abl_fv*, const double*, const double*, double*, cudaStream_t);
 template void run_vjp<2, 2>(abl_fv*, const double*, const double*, double*, cudaStream_t);
+template void run_vjp<2, 3>(abl_fv*, const double*, const double*, double*, cudaStream_t);
 template void run_vjp<3, 0>(abl_fv*, const double*, const double*, double*, cudaStream_t);
 }  // namespace abl

@@ -12,4 +12,7 @@ template void run_jvp<2, 0>(abl_fv*, const double*, const double*, double*, doub
 template void run_rhs<2, 2>(abl_fv*, const double*, double*, int, int, cudaStream_t);
 template void run_aux<2, 2>(abl_fv*, const double*, cudaStream_t);
 template void run_jvp<2, 2>(abl_fv*, const double*, const double*, double*, double*, cudaStream_t);
+template void run_rhs<2, 3>(abl_fv*, const double*, double*, int, int, cudaStream_t);
+template void run_aux<2, 3>(abl_fv*, const double*, cudaStream_t);
+template void run_jvp<2, 3>(abl_fv*, const double*, const double*, double*, double*, cudaStream_t);
 }  // namespace abl

@@ -796,7 +796,7 @@ __device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* n
 
 // ---------------------------------------------------------------------------------------------------
 // One CTA per tile. Phase 1: face fluxes into shared memory (tile-ordered geometry streamed from HBM).
-// Phase 2: each tile cell adds -+flux/V of its faces in ascending face order and writes F once.
+// Phase 2: each tile cell sums -+flux of its faces in ascending face order, adds the sum / V and writes F once.
 template <int DIM, int NS, class G, int FK>
 __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMesh M, Phys P, const double* __restrict__ U,
                                                                      const double* __restrict__ dU, const double* __restrict__ aux,
@@ -839,18 +839,26 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
                     acc[k] = F[(size_t)c * D::NC + k];
             }
         }
+        // the signed face fluxes summed first, then scaled by 1/V once: equal and opposite fluxes cancel
+        // exactly (a uniform state keeps a zero residual, as the reference's per-face division gives;
+        // a per-face fma(flux, 1/V, acc) would leave the rounding error of the product instead)
+        S sum[D::NC];
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) sum[k] = 0.0;
         const int e0 = M.tc_fptr[j], e1 = M.tc_fptr[j + 1];
         for (int e = e0; e < e1; e++) {
             const uint16_t code = M.tc_face[e];
             const S* ff = sflux + (size_t)(code & 0x7fff) * D::NC;
             if (code & 0x8000) {
 #pragma unroll
-                for (int k = 0; k < D::NC; k++) acc[k] += ff[k] * iv;
+                for (int k = 0; k < D::NC; k++) sum[k] += ff[k];
             } else {
 #pragma unroll
-                for (int k = 0; k < D::NC; k++) acc[k] -= ff[k] * iv;
+                for (int k = 0; k < D::NC; k++) sum[k] -= ff[k];
             }
         }
+#pragma unroll
+        for (int k = 0; k < D::NC; k++) acc[k] += sum[k] * iv;
 #pragma unroll
         for (int k = 0; k < D::NC; k++) {
             if constexpr (std::is_same<S, Dual>::value) {

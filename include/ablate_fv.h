@@ -133,7 +133,9 @@ typedef struct abl_physics_desc {
     int32_t eos;             /* ABL_EOS_* */
     double gamma;            /* perfect gas: specific heat ratio (default 1.4) */
     double r_gas;            /* perfect gas: gas constant J/(kg K) (default 287) */
-    int32_t n_species;       /* densityYi components; 0 = no species field */
+    int32_t n_species;       /* densityYi components; 0 = no species field. Compiled (dim, n_species):
+                                (1, 0), (2, 0), (2, 2), (2, 3), (3, 0), (3, 2), (3, 5), (3, 9); others give
+                                ABL_ERR_UNSUPPORTED at create */
     const double* nasa7;     /* [n_species][15]: T_mid, low a1..a7, high a1..a7 (cp/R = a1 + a2 T + ... ) */
     const double* mw;        /* [n_species] molar mass kg/kmol */
 
