@@ -6,7 +6,6 @@ is raised -- there is no fallback implementation.
 from __future__ import annotations
 
 import ctypes as C
-import os
 from pathlib import Path
 
 import numpy as np

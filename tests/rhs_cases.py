@@ -8,7 +8,7 @@ import numpy as np
 from ablate_b200 import _lib as L
 from ablate_b200 import fv, workloads
 from ablate_b200.mesh import box_mesh
-from ablate_b200.workloads import Workload, fill_outflow_ghosts, mixture_state, synthetic_mixture, tgv_state
+from ablate_b200.workloads import Workload, fill_outflow_ghosts, mixture_state, synthetic_mixture
 
 
 def _perturbed_state(mesh, rng, dim, ns=0, eos=None):

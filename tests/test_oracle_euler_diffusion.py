@@ -1,8 +1,6 @@
 """The oracle against the reference's 1D conduction convergence test
 (compressibleFlowEulerDiffusionTests.cpp): order 2.25 for rho E (L2 and Linf, within 0.2), rho and
 rho u exact. In 1D the face gradient comes from the two-cell LeastSquares stencil, so this pins it."""
-import numpy as np
-
 from ablate_b200.workloads import initial_aux
 from oracle import oracle as orc
 from tests import euler_diffusion as ED
