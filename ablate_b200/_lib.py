@@ -132,7 +132,24 @@ def _load():
     return lib
 
 
-lib = _load()
+_LIB = None
+
+
+def get():
+    """The loaded library, mapped on the first call (importing the package maps nothing, so code that
+    only builds meshes, workloads or physics descriptors -- the oracle's CPU runs among them -- never
+    loads the CUDA library)."""
+    global _LIB
+    if _LIB is None:
+        _LIB = _load()
+    return _LIB
+
+
+def __getattr__(name):
+    # `_lib.lib` loads the library on first use
+    if name == "lib":
+        return get()
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 class AblateError(RuntimeError):
@@ -143,7 +160,7 @@ class AblateError(RuntimeError):
 
 def check(rc: int, what: str = ""):
     if rc != OK:
-        msg = lib.abl_last_error_string().decode(errors="replace")
+        msg = get().abl_last_error_string().decode(errors="replace")
         raise AblateError(rc, f"{what}: {msg}" if what else msg)
 
 
@@ -170,5 +187,5 @@ def u8ptr(a: np.ndarray | None):
 
 def device_count() -> int:
     n = C.c_int(0)
-    rc = lib.abl_device_count(C.byref(n))
+    rc = get().abl_device_count(C.byref(n))
     return n.value if rc == OK else 0

@@ -82,10 +82,14 @@ def build_oracle(force: bool = False, verbose: bool = False) -> Path:
     return ORACLE_LIB
 
 
-def build_reference_flux(verbose: bool = False) -> Path | None:
-    """Compile the reference's own flux-calculator sources (oracle/Makefile `ref` target) when the
-    reference checkout is present; the result is a checker for the oracle, never a product path."""
-    ref = Path(os.environ.get("ABLATE_REFERENCE", "/root/reference"))
+def build_reference_flux(ref: str | Path | None = None, verbose: bool = False) -> Path | None:
+    """Compile the reference's own flux-calculator sources (oracle/Makefile `ref` target) from the
+    reference checkout `ref` (default: the ABLATE_REFERENCE environment variable) when one is given and
+    present; the result is a checker for the oracle, never a product path."""
+    ref = ref or os.environ.get("ABLATE_REFERENCE")
+    if not ref:
+        return None
+    ref = Path(ref)
     if not (ref / "src" / "finiteVolume" / "fluxCalculator" / "ausm.cpp").exists():
         return None
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "ref", f"REF={ref}"], check=True)
@@ -96,7 +100,7 @@ def main(argv: list[str]) -> int:
     force = "--force" in argv
     verbose = "-v" in argv
     build_oracle(force, verbose)
-    build_reference_flux(verbose)
+    build_reference_flux(verbose=verbose)
     build_product(force, verbose)
     print(f"built {LIB} and {ORACLE_LIB}")
     return 0

@@ -7,7 +7,6 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
-#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -66,7 +65,8 @@ double host_h_molar(const double* c, double T) {
 void validate_physics(const abl_physics_desc* p) {
     if (!p) throw std::invalid_argument("physics descriptor is NULL");
     if (p->eos != ABL_EOS_PERFECT_GAS && p->eos != ABL_EOS_NASA7) throw std::invalid_argument("unknown eos");
-    if (p->n_species < 0 || p->n_species > 64) throw std::invalid_argument("n_species out of range");
+    if (p->n_species < 0 || p->n_species > kMaxSpecies)
+        throw std::invalid_argument("n_species out of range (0.." + std::to_string(kMaxSpecies) + ")");
     if (p->eos == ABL_EOS_NASA7 && (p->n_species < 1 || !p->nasa7 || !p->mw)) throw std::invalid_argument("NASA-7 EOS needs n_species >= 1, nasa7 and mw");
     if (p->eos == ABL_EOS_PERFECT_GAS && !(p->gamma > 1.0 && p->r_gas > 0.0)) throw std::invalid_argument("perfect gas needs gamma > 1 and r_gas > 0");
     if (p->flux < ABL_FLUX_OFF || p->flux > ABL_FLUX_RIEMANN) throw std::invalid_argument("unknown flux calculator");
@@ -199,7 +199,7 @@ __device__ void eos_property(const Phys& P, int ns, int prop, const double* U, b
             *out = internal_energy<DIM>(U);
             return;
         }
-        Tin = temperature<DIM, 64>(P, ns, U, 300.0, ok);
+        Tin = temperature<DIM, kMaxSpecies>(P, ns, U, 300.0, ok);
         if (prop == ABL_PROP_TEMPERATURE) {
             *out = Tin;
             return;
@@ -226,11 +226,11 @@ __device__ void eos_property(const Phys& P, int ns, int prop, const double* U, b
         }
         return;
     }
-    double ys[64];
+    double ys[kMaxSpecies];
     fill_y(ns, rho, U + 2 + DIM, ys);
     switch (prop) {
         case ABL_PROP_PRESSURE: *out = rho * kRuniv * T / mixture_mw(P, ns, ys); return;
-        case ABL_PROP_TEMPERATURE: *out = temperature<DIM, 64>(P, ns, U, T, ok); return;
+        case ABL_PROP_TEMPERATURE: *out = temperature<DIM, kMaxSpecies>(P, ns, U, T, ok); return;
         case ABL_PROP_INTERNAL_SENSIBLE_ENERGY: *out = e_sens(P, ns, ys, T); return;
         case ABL_PROP_SENSIBLE_ENTHALPY: {
             double h = 0;
@@ -260,7 +260,7 @@ __global__ void k_eos_batch(Phys P, int ns, int prop, int64_t n, const double* c
     if (i >= n) return;
     const int nc = 2 + DIM + ns;
     const int psz = prop == ABL_PROP_SPECIES_SENSIBLE_ENTHALPY ? ns : 1;
-    double u[2 + 3 + 64];
+    double u[2 + 3 + kMaxSpecies];
     for (int k = 0; k < nc; k++) u[k] = conserved[i * nc + k];
     bool ok = true;
     eos_property<DIM>(P, ns, prop, u, T_in != nullptr, T_in ? T_in[i] : 0.0, out + i * psz, &ok);
@@ -284,21 +284,15 @@ constexpr int kNoAllocMaxSpecies = 64;
 constexpr size_t kNoAllocScratchBytes = 16384;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_noalloc_mutex;
-void* g_noalloc_address[256] = {};
-
-// Device address of g_noalloc_scratch on the current device, resolved once per device (host code
-// cannot use the symbol itself: on the host it names a stand-in, not device memory).
-unsigned char* noalloc_scratch(int device) {
-    if (device < 0 || device >= 256) throw std::invalid_argument("device index out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_address[device]) {
-        void* ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr) throw AblError(ABL_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_noalloc_address[device] = ptr;
-    }
-    return static_cast<unsigned char*>(g_noalloc_address[device]);
+// Device address of g_noalloc_scratch on the current device (host code cannot use the symbol itself:
+// on the host it names a stand-in, not device memory). Looked up on every call, so a new context after
+// a cudaDeviceReset gets its own address; the lookup allocates nothing, though on first use it may make
+// CUDA load this library's device code.
+unsigned char* noalloc_scratch() {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) throw AblError(ABL_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return static_cast<unsigned char*>(ptr);
 }
 
 // =================================================================================================
@@ -346,9 +340,15 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         *out = nullptr;
         validate_physics(physics);
         if (!mesh) throw std::invalid_argument("mesh descriptor is NULL");
+        if (mesh->dim < 1 || mesh->dim > 3) throw std::invalid_argument("invalid mesh descriptor: dim must be 1, 2 or 3");
         if (!rhs_supported(mesh->dim, physics->n_species))
             throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for dim " + std::to_string(mesh->dim) + " with " +
                                                     std::to_string(physics->n_species) + " species");
+        const bool lsq = physics->reconstruction == ABL_RECON_LEASTSQUARES;
+        const bool dif = (physics->diffusion || (physics->species_diffusion && physics->n_species > 0)) && physics->transport != ABL_TRANSPORT_NONE;
+        // the descriptor is checked and set up on the host first, so a corrupt mesh is rejected the same
+        // way with or without a device
+        HostMesh h = build_host_mesh(mesh, lsq, dif);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw AblError(ABL_ERR_NO_DEVICE, "no CUDA device visible");
         if (device < 0 || device >= ndev) throw std::invalid_argument("device index out of range");
@@ -356,9 +356,6 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         std::unique_ptr<abl_fv> fv(new abl_fv);
         fv->device = device;
         fv->phys = make_phys(physics);
-        const bool lsq = physics->reconstruction == ABL_RECON_LEASTSQUARES;
-        const bool dif = (physics->diffusion || (physics->species_diffusion && physics->n_species > 0)) && physics->transport != ABL_TRANSPORT_NONE;
-        HostMesh h = build_host_mesh(mesh, lsq, dif);
         fv->dim = h.dim;
         fv->ns = physics->n_species;
         fv->nc = 2 + h.dim + fv->ns;
@@ -964,11 +961,11 @@ int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property
         if (ns > kNoAllocMaxSpecies)
             throw std::invalid_argument("abl_eos_batch_noalloc: " + std::to_string(ns) + " species exceed the " +
                                         std::to_string(kNoAllocMaxSpecies) + " its static scratch holds");
+        // resolved before the n == 0 return, so a zero-length call loads the device code ahead of a pool
+        // allocator's reservation
+        unsigned char* scratch = noalloc_scratch();
         if (n == 0) return;
-        int device = 0;
-        ABL_CUDA(cudaGetDevice(&device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        unsigned char* scratch = noalloc_scratch(device);
         // layout: nasa7 [ns][15] | mw [ns] | 1/mw [ns] | h_ref [ns] | status (int)
         double* d_nasa7 = reinterpret_cast<double*>(scratch);
         double* d_mw = d_nasa7 + 15 * kNoAllocMaxSpecies;

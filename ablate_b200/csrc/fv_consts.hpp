@@ -7,4 +7,8 @@ namespace abl {
 // 2 * kColorCap threads).
 constexpr int kColorCap = 128;
 
+// Largest species count a physics descriptor may carry (the per-thread scratch of the EOS batch
+// kernels is sized by it).
+constexpr int kMaxSpecies = 128;
+
 }  // namespace abl

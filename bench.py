@@ -64,6 +64,44 @@ def make_workload(name, n):
     return workloads.shear3d(n or 256, 5)
 
 
+def workload_for(args, world, rank):
+    """(workload, local domain or None) of this rank. At N > 1 the Taylor-Green box is (128 N) x 128 x 128
+    cut in x-slabs and every rank holds its slab with a two-layer halo. Building it maps no library."""
+    if world > 1:
+        if args.workload != "tgv3d":
+            raise SystemExit("multi-GPU runs partition the tgv3d case")
+        from ablate_b200.workloads import tgv3d_slab
+        dom, w = tgv3d_slab(args.n or 128, world, rank)
+        return w, dom
+    return make_workload(args.workload, args.n), None
+
+
+def workload_config(w, world):
+    """The `config` object of the bench line, identical for both arms (built from the workload alone)."""
+    n_cells = int(w.mesh.n_interior)
+    return {"workload": w.name, "n_cells": world * n_cells, "cells_per_gpu": n_cells, "n_faces": int(w.mesh.n_faces),
+            "description": w.description,
+            "parallelism": (f"dp{world}: x-slab partition, 2-layer halo exchanged over NCCL point-to-point before every RHS"
+                            if world > 1 else "single GPU"),
+            "l2": "flushed (256 MiB write) between timed steps, outside the timed events"}
+
+
+def block_errors(F, F_ref, owned, dim):
+    """Norm-wise relative error ||F - F_ref||_2 / ||F_ref||_2 and the largest absolute difference, per
+    field block (euler, densityYi) over the owned cells."""
+    neul = 2 + dim
+    a, b = F[owned], F_ref[owned]
+    out = {}
+    for name, sl in (("euler", slice(0, neul)), ("densityYi", slice(neul, None))):
+        x, y = a[:, sl], b[:, sl]
+        if x.shape[1] == 0:
+            continue
+        d = x - y
+        out[name] = {"rel_l2": float(np.linalg.norm(d) / max(np.linalg.norm(y), 1e-300)), "max_abs": float(np.abs(d).max()),
+                     "max_abs_ref": float(np.abs(y).max())}
+    return out
+
+
 def algorithmic_bytes(w):
     """Compulsory traffic of one RHS: read the FP64 state once, write the residual once, read 1/V per
     owned cell; per face with an owned side read two int32 cell indices and the FP64 area normal."""
@@ -290,10 +328,14 @@ def cpu_baseline(w, phys, seconds):
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's RHS algorithm (the reference itself needs
+    PETSc, MPI, Kokkos and TChem) on all host cores, rank 0 only. It builds the same workload and config
+    as the GPU arm without mapping the CUDA library (the package loads it on first use only)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    w = make_workload(args.workload, args.n)
+    w, dom = workload_for(args, world, 0)
     phys, keep = w.physics()
     from oracle import oracle as orc
     from ablate_b200.workloads import initial_aux
@@ -308,13 +350,16 @@ def run_reference(args):
     for _ in range(args.steps):
         R(w.U, aux, F, threads)
     t = (time.perf_counter() - t0) / args.steps
-    value = w.mesh.n_interior / t / 1e6
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+    R.close()
+    n_cells = int(w.mesh.n_interior)
+    value = n_cells / t / 1e6
+    sample = (f"one full RHS of the workload per step, {threads} OpenMP threads" if world == 1 else
+              f"one RHS of rank 0's slab ({n_cells} owned cells, its 2-layer halo included) per step, {threads} OpenMP threads; "
+              "the host's cores are shared by all ranks, so the rate of one slab is the host's rate")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "n_cells": int(w.mesh.n_interior), "n_faces": int(w.mesh.n_faces), "description": w.description},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"one full RHS per step, {threads} OpenMP threads"},
+            "dtype": "f64", "data": "synthetic", "config": workload_config(w, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -342,16 +387,12 @@ def main():
     from ablate_b200.workloads import initial_aux
 
     drhs = None
-    if world > 1:
-        if args.workload != "tgv3d":
-            raise SystemExit("multi-GPU runs partition the tgv3d case")
+    w, dom = workload_for(args, world, rank)
+    if dom is not None:
         from ablate_b200.distributed import DistributedRHS
-        from ablate_b200.workloads import tgv3d_slab
-        dom, w = tgv3d_slab(args.n or 128, world, rank)
         drhs = DistributedRHS(dom, w.eos, w.processes, w.petscfv_type, w.limiter, device=local)
         solver = drhs.solver
     else:
-        w = make_workload(args.workload, args.n)
         solver = w.solver(device=local)
     solver.SetAux(initial_aux(w))
     U = torch.from_numpy(w.U).to(dev)
@@ -481,20 +522,24 @@ def main():
         grad, comp = wall_studies(w, solver, U, stream, dev)
         wall = {"functional_gradient": grad, "implicit_vs_explicit": comp}
 
+    # the residuals of this workload's state at each precision (for the accuracy figures below); the
+    # mixture EOS's resident temperatures are reset to the oracle's starting guess first
+    F_dev = {}
+    for prec in (L.PRECISION_FP64, L.PRECISION_MIXED):
+        if prec in results or (prec == L.PRECISION_FP64 and L.PRECISION_MIXED in results):
+            solver.SetAux(initial_aux(w))
+            Fx = torch.zeros_like(U)
+            if drhs is not None:
+                drhs.ComputeRHSDevice(0.0, U, Fx, prec)
+            else:
+                solver.ComputeRHSDevice(0.0, U.data_ptr(), Fx.data_ptr(), prec, stream.cuda_stream)
+            torch.cuda.synchronize(dev)
+            F_dev[prec] = Fx.cpu().numpy()
+    owned_np = w.mesh.cell_kind == L.CELL_OWNED
     # accuracy of the mixed path against FP64 on this workload
     mixed_err = None
-    if L.PRECISION_MIXED in results:
-        F64 = torch.zeros_like(U)
-        F32 = torch.zeros_like(U)
-        solver.ComputeRHSDevice(0.0, U.data_ptr(), F64.data_ptr(), L.PRECISION_FP64, stream.cuda_stream)
-        solver.ComputeRHSDevice(0.0, U.data_ptr(), F32.data_ptr(), L.PRECISION_MIXED, stream.cuda_stream)
-        torch.cuda.synchronize(dev)
-        owned = torch.from_numpy(w.mesh.cell_kind == L.CELL_OWNED).to(dev)
-        neul = 2 + w.mesh.dim
-        a, b = F32[owned], F64[owned]
-        mixed_err = {"euler": float((a[:, :neul] - b[:, :neul]).norm() / b[:, :neul].norm())}
-        if a.shape[1] > neul:
-            mixed_err["densityYi"] = float((a[:, neul:] - b[:, neul:]).norm() / b[:, neul:].norm())
+    if L.PRECISION_MIXED in F_dev:
+        mixed_err = {k: v["rel_l2"] for k, v in block_errors(F_dev[L.PRECISION_MIXED], F_dev[L.PRECISION_FP64], owned_np, w.mesh.dim).items()}
 
     # end to end through the public host API: pinned host buffers, H2D of U and F, RHS, D2H of F
     head = L.PRECISION_FP64 if L.PRECISION_FP64 in results else precisions[0]
@@ -544,11 +589,9 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if head == L.PRECISION_FP64 else "mixed f32/f64", "data": "synthetic",
-        "config": {"workload": w.name, "n_cells": world * n_cells, "cells_per_gpu": n_cells, "n_faces": int(w.mesh.n_faces), "description": w.description,
-                   "parallelism": (f"dp{world}: x-slab partition, 2-layer halo exchanged over NCCL point-to-point before every RHS "
-                                   f"({drhs.halo.bytes_per_exchange} B per rank per step)") if world > 1 else "single GPU",
-                   "l2": "flushed (256 MiB write) between timed steps, outside the timed events",
-                   "record_classes": dict(zip(("cone_weights", "face_geometry"), solver.RecordClasses()))},
+        "config": workload_config(w, world),
+        "layout": {"record_classes": dict(zip(("cone_weights", "face_geometry"), solver.RecordClasses())),
+                   "halo_bytes_per_rank_per_step": drhs.halo.bytes_per_exchange if drhs is not None else 0},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": dom_achieved, "peak": peak, "unit": "GB/s", "frac": dom_achieved / peak,
                      "traffic": read_traffic(w.name, "fp64" if head == L.PRECISION_FP64 else "mixed", dom_name, n_cells) if world == 1 else None,
                      "algorithmic_bytes_per_launch": B, "kernel_ms": dom_ms,
@@ -576,6 +619,13 @@ def main():
         phys, keep = w.physics()
         cb, F_cpu = cpu_baseline(w, phys, args.cpu_seconds)
         line["cpu_baseline"] = cb
+        # every number above states its error against the oracle's FP64 residual of the same state
+        parity = {"reference": "oracle: CPU restatement of the reference RHS, FP64, same seeded state"}
+        if L.PRECISION_FP64 in F_dev:
+            parity["fp64_vs_oracle"] = block_errors(F_dev[L.PRECISION_FP64], F_cpu, owned_np, w.mesh.dim)
+        if L.PRECISION_MIXED in F_dev:
+            parity["mixed_vs_oracle"] = block_errors(F_dev[L.PRECISION_MIXED], F_cpu, owned_np, w.mesh.dim)
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     solver.close()

@@ -273,10 +273,14 @@ int abl_eos_batch(const abl_physics_desc* physics, int dim, int property, int64_
  * cudaFree or allocating library routine: conserved_dev[n][nc], T_dev[n] (or NULL) and out_dev[n][property
  * size] are the caller's device buffers, and the NASA-7 tables and the status word live in a 16 KiB
  * file-scope device array of the library (held by every GPU that loads it until exit), which limits
- * n_species to 64. Work is ordered on `stream`; the call waits for it to finish to return the status.
- * The first call on a device resolves the array's device address and should come before any stream
- * capture. Every call reuses the same array: calls that overlap on the GPU (other streams, other host
- * threads) race on it. */
+ * n_species to 64 (abl_eos_batch takes up to 128); more are rejected with ABL_ERR_INVALID_ARGUMENT.
+ * Work is ordered on `stream`; the call waits for it to finish to return the status.
+ * Every call, n = 0 included, first looks up the array's device address on the current device. That
+ * lookup may load the library's device code on first use (CUDA loads modules lazily by default), which
+ * needs device memory: make one call with n = 0 on each device before a pool allocator reserves the
+ * memory. The call copies the tables from host memory and synchronises `stream`, so it must not be made
+ * while `stream` is being captured into a CUDA graph. Every call reuses the same array: calls that
+ * overlap on the GPU (other streams, other host threads) race on it. */
 int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property, int64_t n, const double* conserved_dev,
                           const double* T_dev, double* out_dev, void* stream);
 

@@ -9,7 +9,8 @@
  * by tests/golden/make_golden.py from the reference test sources). The PETSc pieces the reference
  * calls but does not contain (PetscFVComputeGradient least squares, PetscLimiterLimit,
  * DMPlexComputeGeometryFVM) and TChem's NASA-7 functions are restated from their published
- * algorithms; which of them the reference tests pin is recorded in DESIGN.md.
+ * algorithms; the PETSc LSQ gradient is pinned by exactness on linear fields, the limiter forms by
+ * the reference's least-squares convergence orders, the NASA-7 functions by the gri30 known answers.
  */
 #ifndef ABLATE_ORACLE_H
 #define ABLATE_ORACLE_H

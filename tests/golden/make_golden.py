@@ -3,7 +3,7 @@
 Reads the ABLATE unit-test sources as text (it does not build or run them) and writes
 ``tests/golden/*.json``. Run it where the reference checkout is available:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 Sources read (ABLATE 0.13.03):
   tests/unitTests/finiteVolume/fluxCalculator/fluxCalculatorTests.cpp:56-403
@@ -248,7 +248,10 @@ def shock_tube(ref: Path) -> dict:
 
 
 def main(argv):
-    ref = Path(argv[1] if len(argv) > 1 else "/root/reference")
+    if len(argv) < 2:
+        print("usage: python tests/golden/make_golden.py <reference checkout>", file=sys.stderr)
+        return 2
+    ref = Path(argv[1])
     out = {
         "flux_calculators.json": flux_calculators(ref),
         "ns_transport.json": ns_transport(ref),

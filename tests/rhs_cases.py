@@ -102,6 +102,13 @@ def case(name: str) -> Workload:
         tr = fv.Constant(k=0.03, mu=2e-5, diff=1e-4)
         procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
         return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
+    if name == "shear3d_ns5":
+        # the 256^3 five-species shear layer's generator (outflow ghosts in y, NASA-7, AUSM+up, LSQ +
+        # minmod) at 16^3, large enough for its record tables (7 cone-weight and 4 geometry classes)
+        return workloads.shear3d(16, 5)
+    if name == "wall3d_channel":
+        # the walled channel of the derivative studies (inlet, outflow, no-slip walls, periodic z)
+        return workloads.wall3d(10)
     if name.startswith("tets3d_"):
         # seeded Delaunay tets of the 1 x 0.2 x 0.2 channel: variable cone sizes, ghosts on every side
         if name == "tets3d_ns9":
@@ -136,6 +143,8 @@ CASES = [
     "pgspecies3d_ns2",
     "tets3d_ns9",
     "tets3d_pg_minmod",
+    "shear3d_ns5",
+    "wall3d_channel",
 ]
 
 

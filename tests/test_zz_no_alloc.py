@@ -67,7 +67,17 @@ def test_noalloc_matches_allocating_batch_twice():
 
 
 def test_noalloc_rejects_more_species_than_its_scratch_holds():
+    # 65 species pass the descriptor check (up to 128) and reach the entry point's own limit
     pg = G.perfect_gas_physics(1.4, 287.0, ns=65)
     rc = L.lib.abl_eos_batch_noalloc(C.byref(pg), 3, L.PROP_PRESSURE, 1, C.c_void_p(1), None, C.c_void_p(1), None)
     assert rc == L.ERR_INVALID_ARGUMENT
-    assert b"species" in L.lib.abl_last_error_string()
+    assert b"its static scratch holds" in L.lib.abl_last_error_string()
+
+
+def test_noalloc_zero_length_call_is_a_warm_up():
+    # n = 0 resolves the scratch address (and so loads the device code) without launching anything
+    torch = pytest.importorskip("torch")
+    torch.cuda.set_device(0)
+    pg = G.perfect_gas_physics(1.4, 287.0)
+    rc = L.lib.abl_eos_batch_noalloc(C.byref(pg), 3, L.PROP_PRESSURE, 0, None, None, None, None)
+    L.check(rc, "abl_eos_batch_noalloc warm-up")
