@@ -106,7 +106,7 @@ def case(name: str) -> Workload:
         # the 256^3 five-species shear layer's generator (outflow ghosts in y, NASA-7, AUSM+up, LSQ +
         # minmod) at 16^3, large enough for its record tables (7 cone-weight and 4 geometry classes)
         return workloads.shear3d(16, 5)
-    if name == "wall3d_channel":
+    if name == "walled_channel3d":
         # the walled channel of the derivative studies (inlet, outflow, no-slip walls, periodic z)
         return workloads.wall3d(10)
     if name.startswith("tets3d_"):
@@ -144,7 +144,7 @@ CASES = [
     "tets3d_ns9",
     "tets3d_pg_minmod",
     "shear3d_ns5",
-    "wall3d_channel",
+    "walled_channel3d",
 ]
 
 
