@@ -78,6 +78,7 @@ SIGNATURES = {
     "abl_fv_destroy": (C.c_int, [C.c_void_p]),
     "abl_fv_sizes": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "abl_fv_record_classes": (C.c_int, [C.c_void_p, _ip, _ip]),
+    "abl_fv_fused_info": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "abl_fv_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
     "abl_fv_jvp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -30,6 +30,13 @@ bool record_tables() {
     return !(v && v[0] == '0');
 }
 
+// the fused one-pass RHS where a tile fits in shared memory (the default); ABL_FV_FUSED=0 keeps the
+// two-pass gradient + tile-flux kernels
+bool fused_enabled() {
+    const char* v = std::getenv("ABL_FV_FUSED");
+    return !(v && v[0] == '0');
+}
+
 int fail(const AblError& e) {
     g_last_error = e.what();
     return e.code;
@@ -355,6 +362,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         ABL_CUDA(cudaSetDevice(device));
         std::unique_ptr<abl_fv> fv(new abl_fv);
         fv->device = device;
+        ABL_CUDA(cudaDeviceGetAttribute(&fv->n_sm, cudaDevAttrMultiProcessorCount, device));
         fv->phys = make_phys(physics);
         fv->dim = h.dim;
         fv->ns = physics->n_species;
@@ -408,6 +416,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             tl = tiles_for(tile);
         }
         fv->tile_smem = (int)((size_t)std::max(tl.max_faces, 1) * nc_ * sizeof(double));
+        std::vector<uint16_t> geo_cls;  // per tile face record its geometry record (kept for the fused tables)
         fv->tile_cell_ptr.upload(tl.cell_ptr.data(), tl.cell_ptr.size());
         fv->tile_cells.upload(tl.cells.data(), tl.cells.size());
         fv->tile_face_ptr.upload(tl.face_ptr.data(), tl.face_ptr.size());
@@ -417,6 +426,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             // once per distinct record where they repeat; the mixed path's 48-byte record holds the
             // normal and the offsets as FP32 pairs
             GeoRecords gr = tile_geometry(tl, record_tables());
+            geo_cls = gr.cls;
             const std::vector<double>& geo = gr.geo;
             const size_t ntf = geo.size() / 10;
             if (!gr.cls.empty()) {
@@ -495,6 +505,28 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                 fv->cv32.upload(f32.data(), f32.size());
             }
             fv->max_cone = maxc;
+            if (fused_enabled() && tl.n_tiles > 0) {
+                std::vector<int32_t> wb(h.n_cells);
+                for (int c = 0; c < h.n_cells; c++) wb[c] = cr.classes ? cr.base[c] : h.cone_ptr[c];
+                FusedTiles ft = fused_tiles(h, tl, wb, geo_cls);
+                const bool nasa = physics->eos == ABL_EOS_NASA7 && fv->ns > 0;
+                for (int q = 0; q < 2; q++) {
+                    fv->fused_smem[q] = fused_smem_bytes(h.dim, fv->nc, fv->naux, q == 0 ? 8 : 4, ft.max_ext, ft.max_grad, ft.max_faces, nasa);
+                    // the mixed path with species runs the FP64 kernels
+                    fv->fused_ok[q] = fv->fused_smem[q] <= kFusedSmemLimit && (q == 0 || fv->ns == 0);
+                }
+                if (fv->fused_ok[0] || fv->fused_ok[1]) {
+                    fv->fz_ext_ptr.upload(ft.ext_ptr.data(), ft.ext_ptr.size());
+                    fv->fz_ext.upload(ft.ext.data(), ft.ext.size());
+                    fv->fz_tile_cls.upload(ft.tile_cls.data(), ft.tile_cls.size());
+                    fv->fz_cls_off.upload(ft.cls_off.data(), ft.cls_off.size());
+                    fv->fz_pool.upload(ft.pool.data(), ft.pool.size());
+                    fv->fz_max_ext = ft.max_ext;
+                    fv->fz_max_grad = ft.max_grad;
+                    fv->fz_max_faces = ft.max_faces;
+                    fv->fz_classes = (int)ft.cls_off.size();
+                }
+            }
         }
         {
             // per cell: sum of its LSQ weights over non-boundary faces, and of its aux weights over all
@@ -672,6 +704,15 @@ int abl_fv_record_classes(const abl_fv* fv, int32_t* weight_classes, int32_t* ge
     if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
     if (weight_classes) *weight_classes = fv->n_cone_classes;
     if (geometry_classes) *geometry_classes = fv->n_geo_classes;
+    return ABL_OK;
+}
+
+int abl_fv_fused_info(const abl_fv* fv, int32_t* fp64, int32_t* mixed, int32_t* classes, int32_t* max_ext) {
+    if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
+    if (fp64) *fp64 = fv->fused_ok[0] ? 1 : 0;
+    if (mixed) *mixed = fv->fused_ok[1] ? 1 : 0;
+    if (classes) *classes = fv->fz_classes;
+    if (max_ext) *max_ext = fv->fz_max_ext;
     return ABL_OK;
 }
 
@@ -872,10 +913,10 @@ int abl_fv_status(abl_fv* fv) {
 
 int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches) {
     if (!fv || !launches) return fail(ABL_ERR_INVALID_ARGUMENT, "NULL argument");
-    (void)precision;
     int n = 0;
     if (fv->need_aux) n++;
-    if (fv->need_state_grad || fv->need_aux_grad) n++;
+    const bool fused = fv->fused_ok[precision == ABL_PRECISION_MIXED && fv->ns == 0 ? 1 : 0];
+    if (!fused && (fv->need_state_grad || fv->need_aux_grad)) n++;
     if (fv->mesh.n_tiles > 0) n++;
     *launches = n;
     return ABL_OK;

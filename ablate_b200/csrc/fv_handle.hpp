@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "fv_adjoint.cuh"
+#include "fv_fused.cuh"
 
 namespace abl {
 
@@ -92,6 +93,13 @@ struct abl_fv {
     abl::DevBuf<uint32_t> tf_slot;
     abl::DevBuf<uint16_t> tf_adj;
     int tile_max_cells = 0, n_nb = 0;
+    // the fused one-pass RHS: per-tile ext cells and class tables; usable per gradient precision
+    // (0: FP64, 1: mixed) when a tile's rows fit in shared memory
+    abl::DevBuf<int> fz_ext_ptr, fz_ext, fz_tile_cls, fz_cls_off, fz_pool;
+    int fz_max_ext = 0, fz_max_grad = 0, fz_max_faces = 0, fz_classes = 0;
+    bool fused_ok[2] = {false, false};
+    size_t fused_smem[2] = {0, 0};
+    int n_sm = 1;
     // optional per-kernel timing of the last evaluation
     bool profile = false;
     int n_marks = 0;

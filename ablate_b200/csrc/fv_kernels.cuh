@@ -223,6 +223,22 @@ __device__ __forceinline__ void load_state(const double* __restrict__ U, int c, 
     load_state<DIM, NS, double>(U, nullptr, c, u);
 }
 
+// aux (T, u, Y) of a perfect-gas cell from its conserved state: T = e / cv with e = E/rho - |u|^2/2
+template <int DIM, int NS, class S>
+__device__ __forceinline__ void aux_from_state(const Phys& P, const S* u, S* a) {
+    using D = Dims<DIM, NS>;
+    const S irho = rcp64(u[0]);
+    S ke = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        a[1 + d] = u[2 + d] * irho;
+        ke += a[1 + d] * a[1 + d];
+    }
+    a[0] = (u[1] * irho - 0.5 * ke) * rcp64(P.r_gas / (P.gamma - 1.0));
+#pragma unroll
+    for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
+}
+
 // aux (T, u, Y) of one cell: from the resident aux array for the mixture EOS, recomputed from the
 // conserved state for a perfect gas (UpdateAuxTemperatureField / UpdateAuxVelocityField /
 // UpdateAuxMassFractionField: navierStokesTransport.cpp:534-558, speciesTransport.cpp:98-110)
@@ -245,17 +261,34 @@ __device__ __forceinline__ void cell_aux(const Phys& P, const S* u, const double
         }
         return;
     }
-    const S irho = rcp64(u[0]);
-    S ke = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-        a[1 + d] = u[2 + d] * irho;
-        ke += a[1 + d] * a[1 + d];
-    }
-    a[0] = (u[1] * irho - 0.5 * ke) * rcp64(P.r_gas / (P.gamma - 1.0));
-#pragma unroll
-    for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
+    aux_from_state<DIM, NS>(P, u, a);
 }
+
+// Where the per-cell rows a face flux reads come from. GlobalRows: the resident arrays by cell index (the
+// two-pass kernels; the tangent kernels also read dU). The fused tile kernel has a shared-memory source
+// by tile-local slot (SharedRows, fv_fused.cuh). Both deliver the same values, so the flux arithmetic is
+// shared and the two paths agree bit for bit.
+template <int DIM, int NS, class G>
+struct GlobalRows {
+    using D = Dims<DIM, NS>;
+    using GR = GradRows<DIM, NS, G>;
+    const double* __restrict__ U;
+    const double* __restrict__ dU;
+    const double* __restrict__ aux;
+    const G* __restrict__ grad;
+    const G* __restrict__ agrad;
+    template <class S>
+    __device__ __forceinline__ void state(int c, S* u) const {
+        load_state<DIM, NS, S>(U, dU, c, u);
+    }
+    __device__ __forceinline__ double temperature(int c) const { return __ldg(aux + (size_t)c * D::NA); }
+    template <class S>
+    __device__ __forceinline__ void aux_of(const Phys& P, const S* u, int c, S* a) const {
+        cell_aux<DIM, NS>(P, u, aux, c, a);
+    }
+    __device__ __forceinline__ void grad_row(int c, G* g) const { load_row<D::NC * DIM, G>(grad + (size_t)c * GR::GS, g); }
+    __device__ __forceinline__ void agrad_row(int c, G* g) const { load_row<D::NA * DIM, G>(agrad + (size_t)c * GR::AS, g); }
+};
 
 // ---------------------------------------------------------------------------------------------------
 template <int DIM, int NS>
@@ -541,18 +574,17 @@ __host__ __device__ __forceinline__ void face_weights_1d(const double* fdx, doub
 
 // ---------------------------------------------------------------------------------------------------
 // flux of one face: advection (NS + species) and diffusion (NS + species), summed per component
-template <int DIM, int NS, class G, int FK>
-__device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L, int R, const double* normal, const double* fdx,
-                                          const double* __restrict__ U, const double* __restrict__ dU, const double* __restrict__ aux,
-                                          const G* __restrict__ grad, const G* __restrict__ agrad, StateOf<G>* flux, bool* ok, bool* rok) {
+// L and R index the rows of `src` (global cells, or tile-local slots of the fused kernel).
+template <int DIM, int NS, class G, int FK, class Src>
+__device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, int R, const double* normal, const double* fdx, StateOf<G>* flux,
+                                          bool* ok, bool* rok) {
     using D = Dims<DIM, NS>;
-    using GR = GradRows<DIM, NS, G>;
     using S = StateOf<G>;
 #pragma unroll
     for (int k = 0; k < D::NC; k++) flux[k] = 0.0;
     S cL[D::NC], cR[D::NC];
-    load_state<DIM, NS, S>(U, dU, L, cL);
-    load_state<DIM, NS, S>(U, dU, R, cR);
+    src.state(L, cL);
+    src.state(R, cR);
     const bool adv = P.advection && P.flux != ABL_FLUX_OFF;
     const bool spadv = NS > 0 && P.sp_adv && P.flux != ABL_FLUX_OFF;
     if (adv || spadv) {
@@ -567,8 +599,8 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
         if (lsq) {
             // cells without a gradient hold a zero row, so u + 0 . dx = u exactly
             G gL[D::NC * DIM], gR[D::NC * DIM];
-            load_row<D::NC * DIM, G>(grad + (size_t)L * GR::GS, gL);
-            load_row<D::NC * DIM, G>(grad + (size_t)R * GR::GS, gR);
+            src.grad_row(L, gL);
+            src.grad_row(R, gR);
 #pragma unroll
             for (int k = 0; k < D::NC; k++) {
                 G dotL = 0, dotR = 0;
@@ -583,8 +615,8 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
         }
         double TL = 300.0, TR = 300.0;
         if (NS > 0 && P.eos == ABL_EOS_NASA7) {
-            TL = __ldg(aux + (size_t)L * D::NA);
-            TR = __ldg(aux + (size_t)R * D::NA);
+            TL = src.temperature(L);
+            TR = src.temperature(R);
         }
         bool split = false;
         if constexpr (std::is_same<G, float>::value) {
@@ -675,8 +707,8 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
         // FaceInterpolant: face value = average of the two cells, face gradient = average of the two
         // cells' least-squares gradients (LeastSquaresAverage with numberStencils = 2)
         S fs[D::NC], fa[D::NA], aL[D::NA], aR[D::NA];
-        cell_aux<DIM, NS>(P, cL, aux, L, aL);
-        cell_aux<DIM, NS>(P, cR, aux, R, aR);
+        src.aux_of(P, cL, L, aL);
+        src.aux_of(P, cR, R, aR);
 #pragma unroll
         for (int k = 0; k < D::NC; k++) fs[k] = cL[k] * 0.5 + cR[k] * 0.5;
 #pragma unroll
@@ -690,8 +722,8 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 #pragma unroll
             for (int k = 0; k < D::NA; k++) gL[k] = gR[k] = static_cast<G>(aL[k] * wl + aR[k] * wr);
         } else {
-            load_row<D::NA * DIM, G>(agrad + (size_t)L * GR::AS, gL);
-            load_row<D::NA * DIM, G>(agrad + (size_t)R * GR::AS, gR);
+            src.agrad_row(L, gL);
+            src.agrad_row(R, gR);
         }
         S mu, kc, diff;
         transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
@@ -763,11 +795,11 @@ __device__ __forceinline__ void face_flux(const DevMesh& M, const Phys& P, int L
 }
 
 // ---------------------------------------------------------------------------------------------------
-// area normal and both sides' offsets of tile face i with vector loads of its geometry record
+// area normal and both sides' offsets of geometry record `rec` with vector loads
 template <int DIM, class G>
-__device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* normal, double* fdx) {
+__device__ __forceinline__ void face_geometry_rec(const DevMesh& M, size_t rec, double* normal, double* fdx) {
     if constexpr (std::is_same<G, float>::value) {
-        const double2* r = reinterpret_cast<const double2*>(M.tf_geo32) + 3 * geo_record(M, i);
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo32) + 3 * rec;
         const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
         const double n[3] = {a.x, a.y, b.x};
 #pragma unroll
@@ -780,7 +812,7 @@ __device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* n
             fdx[2 * q + 1] = double(__int_as_float((int)(bits >> 32)));
         }
     } else {
-        const double2* r = reinterpret_cast<const double2*>(M.tf_geo) + 5 * geo_record(M, i);
+        const double2* r = reinterpret_cast<const double2*>(M.tf_geo) + 5 * rec;
         const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), e = __ldg(r + 3), f = __ldg(r + 4);
         const double n[3] = {a.x, a.y, b.x};
 #pragma unroll
@@ -792,6 +824,11 @@ __device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* n
         fdx[4] = e.y;
         fdx[5] = f.x;
     }
+}
+// the same for tile face record i
+template <int DIM, class G>
+__device__ __forceinline__ void face_geometry(const DevMesh& M, int i, double* normal, double* fdx) {
+    face_geometry_rec<DIM, G>(M, geo_record(M, i), normal, fdx);
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -810,12 +847,13 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
     const int t = t0 + blockIdx.x;
     const int fb = M.tile_face_ptr[t], fe = M.tile_face_ptr[t + 1];
     bool ok = true, rok = true;
+    const GlobalRows<DIM, NS, G> src{U, dU, aux, grad, agrad};
     for (int i = fb + threadIdx.x; i < fe; i += blockDim.x) {
         const int2 lr = M.tf_cells[i];
         double normal[DIM], fdx[6];
         face_geometry<DIM, G>(M, i, normal, fdx);
         S flux[D::NC];
-        face_flux<DIM, NS, G, FK>(M, P, lr.x, lr.y, normal, fdx, U, dU, aux, grad, agrad, flux, &ok, &rok);
+        face_flux<DIM, NS, G, FK>(P, src, lr.x, lr.y, normal, fdx, flux, &ok, &rok);
         S* out = sflux + (size_t)(i - fb) * D::NC;
 #pragma unroll
         for (int k = 0; k < D::NC; k++) out[k] = flux[k];

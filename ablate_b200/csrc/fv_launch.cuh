@@ -41,6 +41,45 @@ void launch_tile(abl_fv* fv, const double* U, const double* dU, const G* grad, c
     }
 }
 
+// the fused one-pass RHS over all tiles, or (host-buffer call) chunk by chunk as launch_tile does
+template <int DIM, int NS, class G, int FK, int LIM>
+void launch_fused(abl_fv* fv, const double* U, double* F, int overwrite, cudaStream_t s) {
+    auto kern = k_fused_rhs<DIM, NS, G, FK, LIM>;
+    const int q = std::is_same<G, float>::value ? 1 : 0;
+    const size_t smem = fv->fused_smem[q];
+    ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const FusedDev T{fv->fz_max_ext, fv->fz_max_grad, fv->fz_max_faces, fv->fz_ext_ptr.p, fv->fz_ext.p, fv->fz_tile_cls.p, fv->fz_cls_off.p,
+                     fv->fz_pool.p};
+    auto run = [&](int ta, int tb) {
+        if (tb <= ta) return;
+        // persistent: one CTA per SM (the shared memory of a tile allows one), each looping over tiles
+        const int grid = std::min(tb - ta, fv->n_sm);
+        kern<<<grid, kFusedThreads, smem, s>>>(fv->mesh, fv->phys, T, U, fv->aux.p, F, overwrite, fv->need_state_grad, fv->need_aux_grad,
+                                               fv->status.p, ta, tb);
+        check_launch();
+    };
+    if (!fv->pipe_active) {
+        run(0, fv->mesh.n_tiles);
+        return;
+    }
+    const int nch = fv->chunk_tile.empty() ? 0 : (int)fv->chunk_tile.size() - 1;
+    if (nch == 0) {
+        ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_in[0], 0));
+        run(0, fv->mesh.n_tiles);
+        return;
+    }
+    for (int c = 0; c < nch; c++) {
+        const int ta = fv->chunk_tile[c], tb = fv->chunk_tile[c + 1];
+        ABL_CUDA(cudaStreamWaitEvent(s, fv->ev_in[c], 0));
+        run(ta, tb);
+        ABL_CUDA(cudaEventRecord(fv->ev_chunk[c], s));
+        ABL_CUDA(cudaStreamWaitEvent(fv->out_stream, fv->ev_chunk[c], 0));
+        const size_t r0 = (size_t)fv->chunk_row[c] * fv->nc, r1 = (size_t)fv->chunk_row[c + 1] * fv->nc;
+        if (r1 > r0)
+            ABL_CUDA(cudaMemcpyAsync(fv->pipe_F_host + r0, F + r0, (r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost, fv->out_stream));
+    }
+}
+
 // shared memory for the neighbour differences the limiter reuses (none when it would not fit)
 template <int DIM, int NS, class G>
 size_t gradient_smem(const abl_fv* fv) {
@@ -61,6 +100,22 @@ void launch_gradient(abl_fv* fv, const double* U, const double* dU, G* grad, G* 
 template <int DIM, int NS, class G>
 void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int overwrite, cudaStream_t s) {
     const Phys& P = fv->phys;
+    if (fv->fused_ok[std::is_same<G, float>::value ? 1 : 0]) {
+        mark(fv, "k_fused_rhs", s);
+        if (fv->mesh.n_tiles > 0) {
+            if (P.flux == ABL_FLUX_AUSMPUP) {
+                if (P.limiter == ABL_LIMITER_MINMOD)
+                    launch_fused<DIM, NS, G, ABL_FLUX_AUSMPUP, ABL_LIMITER_MINMOD>(fv, U, F, overwrite, s);
+                else
+                    launch_fused<DIM, NS, G, ABL_FLUX_AUSMPUP, -1>(fv, U, F, overwrite, s);
+            } else if (P.flux == ABL_FLUX_AUSM) {
+                launch_fused<DIM, NS, G, ABL_FLUX_AUSM, -1>(fv, U, F, overwrite, s);
+            } else {
+                launch_fused<DIM, NS, G, -1, -1>(fv, U, F, overwrite, s);
+            }
+        }
+        return;
+    }
     if (fv->need_state_grad || fv->need_aux_grad) {
         mark(fv, "k_gradient", s);
         if (P.limiter == ABL_LIMITER_MINMOD)

@@ -203,6 +203,7 @@ struct Tiles {
     std::vector<int32_t> cells;           // owned cells grouped by tile
     std::vector<int32_t> face_ptr;        // [n_tiles+1] into the tile-face records
     std::vector<int32_t> tf_cells;        // [ntf][2] global left/right cell
+    std::vector<int32_t> tf_face;         // [ntf] global face
     std::vector<double> tf_normal;        // [ntf][3]
     std::vector<double> tf_fdx;           // [ntf][6] face centroid minus each side's centroid
     std::vector<int32_t> tc_fptr;         // [n_owned+1] per tile cell into tc_face
@@ -289,6 +290,7 @@ inline Tiles build_tiles(const HostMesh& h, const abl_mesh_desc* m, int tile_cel
             const int L = h.face_cells[2 * f], R = h.face_cells[2 * f + 1];
             t.tf_cells.push_back(L);
             t.tf_cells.push_back(R);
+            t.tf_face.push_back(f);
             for (int d = 0; d < 3; d++) t.tf_normal.push_back(d < dim ? m->face_normal[3 * (size_t)f + d] : 0.0);
             for (int z = 0; z < 6; z++) t.tf_fdx.push_back(h.fdx[6 * (size_t)f + z]);
             t.tf_slot.push_back((uint32_t)(local[L] >= 0 ? local[L] : 0xffff) | ((uint32_t)(local[R] >= 0 ? local[R] : 0xffff) << 16));
@@ -632,6 +634,171 @@ inline GeoRecords tile_geometry(const Tiles& tl, bool tables) {
     g.geo.swap(table);
     g.cls.assign(cls.begin(), cls.end());
     return g;
+}
+
+// Order in which a cell sums its faces in the fused kernel: its cone (canonical, by neighbour offset)
+// sorted by the axis of the offset's largest component, then its sign. On a hex cell that is x-, x+,
+// y-, y+, z-, z+: opposite faces are summed next to each other, so equal and opposite fluxes cancel
+// exactly (a uniform state keeps a zero residual). The order depends on the cell's geometry alone, so it
+// is the same in every tile and every partition.
+inline int face_sum_key(const HostMesh& h, int i) {
+    const size_t f = (size_t)h.cone_face[i];
+    const int s = h.cone_side[i];
+    int axis = 0;
+    double best = -1.0, v = 0.0;
+    for (int d = 0; d < h.dim; d++) {
+        const double x = h.fdx[6 * f + 3 * s + d] - h.fdx[6 * f + 3 * (1 - s) + d];  // x_n - x_c
+        if (std::fabs(x) > best) {
+            best = std::fabs(x);
+            axis = d;
+            v = x;
+        }
+    }
+    return 2 * axis + (v > 0 ? 1 : 0);
+}
+
+// Tables of the fused one-pass RHS (k_fused_rhs). Per tile its ext cells: the tile's cells (in tile
+// order), then ring 1 (the cells across the tile's faces), then ring 2 (the further neighbours of
+// ring 1), each ring in the order a walk of the previous one meets them (cells in order, each cone in
+// its canonical order). The tile's faces are listed in the order a walk of its cells' cones meets
+// them, and every tile cell lists its faces in face_sum_key order. All of it follows from the local
+// geometry, so the tiles of a structured block get equal tables; the local topology of a tile (cones,
+// faces, face lists in local slots, kinds, weight and geometry records) is one run of int words, and
+// tiles whose runs are equal word for word share one copy (class).
+struct FusedTiles {
+    int max_ext = 0, max_grad = 0, max_faces = 0;
+    std::vector<int32_t> ext_ptr;   // [n_tiles + 1]
+    std::vector<int32_t> ext;       // global cell per ext slot
+    std::vector<int32_t> tile_cls;  // [n_tiles]
+    std::vector<int32_t> cls_off;   // [n_classes] into pool
+    std::vector<int32_t> pool;
+};
+
+// weight_base[c]: first weight record of cell c's cone (its class copy, or its own cone start);
+// geo_cls: per tile face record its geometry record (empty: the record index itself)
+inline FusedTiles fused_tiles(const HostMesh& h, const Tiles& tl, const std::vector<int32_t>& weight_base, const std::vector<uint16_t>& geo_cls) {
+    FusedTiles ft;
+    std::vector<int32_t> slot(h.n_cells, -1), fidx(h.n_faces, -1), rec_of(h.n_faces, -1);
+    std::vector<int32_t> ext, words, flist;
+    std::vector<std::pair<int, int>> order;
+    std::unordered_multimap<uint64_t, int32_t> seen;
+    ft.ext_ptr.push_back(0);
+    for (int k = 0; k < tl.n_tiles; k++) {
+        const int cb = tl.cell_ptr[k], ce = tl.cell_ptr[k + 1], nt = ce - cb;
+        ext.clear();
+        for (int j = cb; j < ce; j++) {
+            slot[tl.cells[j]] = (int32_t)ext.size();
+            ext.push_back(tl.cells[j]);
+        }
+        // ring 1, then ring 2
+        size_t from = 0;
+        int ng = 0;
+        for (int ring = 0; ring < 2; ring++) {
+            const size_t to = ext.size();
+            for (size_t q = from; q < to; q++) {
+                const int c = ext[q];
+                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) {
+                    const int n = h.cone_nbr[i];
+                    if (slot[n] < 0) {
+                        slot[n] = (int32_t)ext.size();
+                        ext.push_back(n);
+                    }
+                }
+            }
+            if (ring == 0) ng = (int)ext.size();
+            from = to;
+        }
+        const int ne = (int)ext.size();
+        if (ne > 0xffff) throw std::invalid_argument("fused tile has too many ext cells");
+        // the tile's faces in walk order, and each face's record among the tile's face records
+        flist.clear();
+        for (int j = 0; j < nt; j++)
+            for (int i = h.cone_ptr[ext[j]]; i < h.cone_ptr[ext[j] + 1]; i++) {
+                const int f = h.cone_face[i];
+                if (fidx[f] < 0) {
+                    fidx[f] = (int32_t)flist.size();
+                    flist.push_back(f);
+                }
+            }
+        const int fb = tl.face_ptr[k], fe = tl.face_ptr[k + 1], nf = (int)flist.size();
+        if (nf != fe - fb || nf > 0x7fff) throw std::logic_error("fused tile faces differ from the tile's face records");
+        for (int i = fb; i < fe; i++) rec_of[tl.tf_face[i]] = i;
+        words.assign({nt, ng, ne, nf});
+        // cone starts, weight bases, kinds, neighbour slots
+        int acc = 0;
+        for (int j = 0; j < ng; j++) {
+            words.push_back(acc);
+            acc += h.cone_ptr[ext[j] + 1] - h.cone_ptr[ext[j]];
+        }
+        words.push_back(acc);
+        for (int j = 0; j < ng; j++) words.push_back(weight_base[ext[j]]);
+        for (int j = 0; j < ng; j++) words.push_back(h.kind[ext[j]]);
+        for (int j = 0; j < ng; j++) {
+            const int c = ext[j];
+            for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++)
+                words.push_back(slot[h.cone_nbr[i]] | (h.face_boundary[h.cone_face[i]] ? (1 << 16) : 0));
+        }
+        for (int f : flist) {
+            const int L = h.face_cells[2 * (size_t)f], R = h.face_cells[2 * (size_t)f + 1];
+            if (slot[L] < 0 || slot[L] >= ng || slot[R] < 0 || slot[R] >= ng) throw std::logic_error("fused tile face outside ring 1");
+            words.push_back(slot[L] | (slot[R] << 16));
+        }
+        for (int f : flist) {
+            if (rec_of[f] < 0) throw std::logic_error("fused tile face without a record");
+            words.push_back(geo_cls.empty() ? rec_of[f] : (int32_t)geo_cls[rec_of[f]]);
+        }
+        // per tile cell its faces in face_sum_key order: local face | side << 15 (side 1: the cell is the
+        // face's right cell and adds the flux)
+        const size_t tcp0 = words.size();
+        words.resize(words.size() + nt + 1);
+        int ntc = 0;
+        std::vector<int32_t> entries;
+        for (int j = 0; j < nt; j++) {
+            const int c = ext[j];
+            order.clear();
+            for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1]; i++) order.push_back({face_sum_key(h, i), i});
+            std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            words[tcp0 + j] = ntc;
+            for (const auto& o : order) {
+                entries.push_back(fidx[h.cone_face[o.second]] | (h.cone_side[o.second] ? 0x8000 : 0));
+                ntc++;
+            }
+        }
+        words[tcp0 + nt] = ntc;
+        words.insert(words.end(), entries.begin(), entries.end());
+        for (int f : flist) {
+            fidx[f] = -1;
+            rec_of[f] = -1;
+        }
+        for (int i = fb; i < fe; i++) rec_of[tl.tf_face[i]] = -1;
+        for (int c : ext) slot[c] = -1;
+        ft.ext.insert(ft.ext.end(), ext.begin(), ext.end());
+        ft.ext_ptr.push_back((int32_t)ft.ext.size());
+        ft.max_ext = std::max(ft.max_ext, ne);
+        ft.max_grad = std::max(ft.max_grad, ng);
+        ft.max_faces = std::max(ft.max_faces, nf);
+        // one copy per distinct run of words
+        uint64_t hk = 1469598103934665603ull;
+        for (int32_t x : words) {
+            hk = (hk ^ (uint32_t)x) * 1099511628211ull;
+            hk ^= hk >> 29;
+        }
+        int32_t cls = -1;
+        const auto range = seen.equal_range(hk);
+        for (auto it = range.first; it != range.second && cls < 0; ++it) {
+            const int32_t o = ft.cls_off[it->second];
+            const size_t len = (it->second + 1 < (int32_t)ft.cls_off.size() ? (size_t)ft.cls_off[it->second + 1] : ft.pool.size()) - o;
+            if (len == words.size() && std::memcmp(&ft.pool[o], words.data(), len * sizeof(int32_t)) == 0) cls = it->second;
+        }
+        if (cls < 0) {
+            cls = (int32_t)ft.cls_off.size();
+            ft.cls_off.push_back((int32_t)ft.pool.size());
+            ft.pool.insert(ft.pool.end(), words.begin(), words.end());
+            seen.emplace(hk, cls);
+        }
+        ft.tile_cls.push_back(cls);
+    }
+    return ft;
 }
 
 }  // namespace abl

@@ -557,6 +557,13 @@ class FiniteVolumeSolver:
         L.check(L.lib.abl_fv_record_classes(self.handle, C.byref(w), C.byref(g)))
         return w.value, g.value
 
+    def FusedInfo(self) -> dict:
+        """Which RHS kernels the handle runs: the fused one-pass kernel per precision (where a tile fits
+        in shared memory), its distinct tile tables, and the most cells one tile stages."""
+        a, b, c, d = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        L.check(L.lib.abl_fv_fused_info(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
+        return {"fp64": bool(a.value), "mixed": bool(b.value), "tile_classes": c.value, "max_staged_cells": d.value}
+
     def close(self):
         if getattr(self, "handle", None):
             L.lib.abl_fv_destroy(self.handle)

@@ -189,6 +189,13 @@ int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells,
  * create, keeps one record per face and cone entry. */
 int abl_fv_record_classes(const abl_fv* fv, int32_t* weight_classes, int32_t* geometry_classes);
 
+/* The RHS kernel layout of a handle: whether the fused one-pass kernel runs the FP64 and the mixed RHS
+ * (it does where one tile's staged rows, gradients and face fluxes fit in shared memory; otherwise the
+ * gradient pass and the tile flux pass run), how many distinct tile tables it holds, and the largest
+ * number of cells one tile stages (its cells and two rings of neighbours). No counterpart in the
+ * reference: a diagnostic of this backend. */
+int abl_fv_fused_info(const abl_fv* fv, int32_t* fp64, int32_t* mixed, int32_t* classes, int32_t* max_ext);
+
 /* ---- the hot path ----------------------------------------------------------------------------- */
 /* F += RHS(U) for owned cells, device pointers, on `stream` (a cudaStream_t; NULL = legacy stream).
  * Runs the aux update (T, velocity, Y for every local cell, T guess = the resident aux T), the

@@ -2,12 +2,16 @@
 // tests/test_setup_records.py: reads a mesh descriptor from a binary file, builds the host mesh, the
 // tiles and the cone-weight and face-geometry records with and without record tables, and checks
 //   * the canonical cone order: each cell's neighbour offsets x_n - x_c ascend lexicographically;
-//   * that the tables expand back to the one-record-per-item arrays bit for bit.
-// Prints "weight_classes <n> geometry_classes <m> ok <0|1>".
+//   * that the tables expand back to the one-record-per-item arrays bit for bit;
+//   * that the fused kernel's per-tile tables (ext cells, local cones, faces and face lists, shared
+//     between tiles whose tables are equal) decode back to the global mesh, tile by tile.
+// Prints "weight_classes <n> geometry_classes <m> fused_classes <k> max_ext <e> ok <0|1>".
 //
 // File layout (little-endian): int32 dim, n_cells, n_faces, has_shift, lsq, dif; then face_cells
 // (int32 [n_faces][2]), face_normal, face_centroid ([n_faces][3] double), cell_centroid ([n_cells][3]),
 // cell_volume ([n_cells]), cell_kind (uint8 [n_cells]) and, when has_shift, face_shift ([n_faces][3]).
+#include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -82,6 +86,61 @@ int main(int argc, char** argv) {
     } else if (pass) {
         pass = gt.geo == g1.geo;
     }
-    std::printf("weight_classes %zu geometry_classes %zu ok %d\n", tab.classes, gt.cls.empty() ? (size_t)0 : gt.geo.size() / 10, pass ? 1 : 0);
+
+    // the fused tables, decoded tile by tile against the global mesh
+    std::vector<int32_t> wb(nc);
+    for (int c = 0; c < nc; c++) wb[c] = tab.classes ? tab.base[c] : h.cone_ptr[c];
+    const abl::FusedTiles ft = abl::fused_tiles(h, tl, wb, gt.cls);
+    pass = pass && (int)ft.tile_cls.size() == tl.n_tiles && (int)ft.ext_ptr.size() == tl.n_tiles + 1;
+    for (int k = 0; k < tl.n_tiles && pass; k++) {
+        const int32_t* cl = ft.pool.data() + ft.cls_off[ft.tile_cls[k]];
+        const int nt = cl[0], ng = cl[1], ne = cl[2], nf = cl[3];
+        const int32_t* gofs = cl + 4;
+        const int32_t* wbs = gofs + ng + 1;
+        const int32_t* kinds = wbs + ng;
+        const int32_t* nbr = kinds + ng;
+        const int32_t* faces = nbr + gofs[ng];
+        const int32_t* fgeo = faces + nf;
+        const int32_t* tcp = fgeo + nf;
+        const int32_t* tce = tcp + nt + 1;
+        const int32_t* ext = ft.ext.data() + ft.ext_ptr[k];
+        const int cb = tl.cell_ptr[k], fb = tl.face_ptr[k];
+        pass = nt == tl.cell_ptr[k + 1] - cb && nf == tl.face_ptr[k + 1] - fb && ne == ft.ext_ptr[k + 1] - ft.ext_ptr[k] && nt <= ng && ng <= ne;
+        for (int j = 0; j < nt && pass; j++) pass = ext[j] == tl.cells[cb + j];
+        for (int j = 0; j < ng && pass; j++) {
+            const int c = ext[j];
+            pass = gofs[j + 1] - gofs[j] == h.cone_ptr[c + 1] - h.cone_ptr[c] && wbs[j] == wb[c] && kinds[j] == h.kind[c];
+            for (int i = 0; i < gofs[j + 1] - gofs[j] && pass; i++) {
+                const int e = h.cone_ptr[c] + i, w = nbr[gofs[j] + i];
+                pass = (w & 0xffff) < ne && ext[w & 0xffff] == h.cone_nbr[e] && ((w >> 16) != 0) == (h.face_boundary[h.cone_face[e]] != 0);
+            }
+        }
+        // the faces are the tile's face records in another order: compare (left, right, geometry) multisets
+        std::vector<std::array<int, 3>> a, b;
+        for (int i = 0; i < nf && pass; i++) {
+            const int lr = faces[i];
+            pass = (lr & 0xffff) < ng && (lr >> 16) < ng;
+            if (pass) a.push_back({ext[lr & 0xffff], ext[lr >> 16], fgeo[i]});
+        }
+        for (int i = 0; i < nf && pass; i++)
+            b.push_back({tl.tf_cells[2 * (size_t)(fb + i)], tl.tf_cells[2 * (size_t)(fb + i) + 1], gt.cls.empty() ? fb + i : (int)gt.cls[fb + i]});
+        std::sort(a.begin(), a.end());
+        std::sort(b.begin(), b.end());
+        pass = pass && a == b;
+        // each tile cell lists each of its faces once, on its own side, opposite faces next to each other
+        for (int j = 0; j < nt && pass; j++) {
+            const int c = ext[j];
+            pass = tcp[j + 1] - tcp[j] == h.cone_ptr[c + 1] - h.cone_ptr[c];
+            std::vector<int> seenf;
+            for (int e = tcp[j]; e < tcp[j + 1] && pass; e++) {
+                const int code = tce[e], fi = code & 0x7fff, lr = faces[fi];
+                pass = fi < nf && ext[(code & 0x8000) ? (lr >> 16) : (lr & 0xffff)] == c &&
+                       std::find(seenf.begin(), seenf.end(), fi) == seenf.end();
+                seenf.push_back(fi);
+            }
+        }
+    }
+    std::printf("weight_classes %zu geometry_classes %zu fused_classes %zu max_ext %d ok %d\n", tab.classes,
+                gt.cls.empty() ? (size_t)0 : gt.geo.size() / 10, ft.cls_off.size(), ft.max_ext, pass ? 1 : 0);
     return pass ? 0 : 1;
 }

@@ -42,6 +42,8 @@ def _run(checker, tmp_path, mesh, lsq=True, dif=True):
     r = subprocess.run([str(checker), str(p)], capture_output=True, text=True)
     words = r.stdout.split()
     assert r.returncode == 0 and words[-1] == "1", r.stdout + r.stderr
+    fields = dict(zip(words[0::2], words[1::2]))
+    _run.last = {k: int(v) for k, v in fields.items()}
     return int(words[1]), int(words[3])
 
 
@@ -49,6 +51,9 @@ def test_periodic_box_has_one_weight_class_and_three_geometry_classes(checker, t
     # every cell of a periodic box sees the same neighbours in the same order: one weight sequence;
     # the tile faces have three orientations
     assert _run(checker, tmp_path, box_mesh((16, 16, 16), periodic=(True, True, True), order="morton")) == (1, 3)
+    # every 8x8x4 tile of the periodic box has the same local topology: one fused table; it stages its
+    # 256 cells, 256 ring-1 and 336 ring-2 cells
+    assert _run.last["fused_classes"] == 1 and _run.last["max_ext"] == 848
 
 
 def test_walled_box_has_a_few_classes(checker, tmp_path):
