@@ -33,17 +33,20 @@ template <class R>
 ABL_HD R sqr(R a) { return a * a; }
 
 // FP64 reciprocal: the hardware approximation of PTX rcp.approx.ftz.f64 (relative error about 2^-23)
-// refined by two Newton-Raphson steps r <- r (2 - x r), each squaring the relative error, to below one
-// ulp. Zero, infinite, NaN and extreme inputs (|x| outside 1e-300..1e300, where the approximation
-// flushes subnormals) take the IEEE division, so their special values are exactly those of 1/x.
+// refined by two Newton-Raphson steps in residual form, e = 1 - x r by one fused multiply-add and
+// r <- r + r e by another (Markstein, "IA-64 and Elementary Functions", 2000, ch. 8): the first step
+// squares the relative error to about 2^-46, the second's residual is exact and leaves the result within
+// one ulp of 1/x (mostly the correctly rounded value). Zero, infinite, NaN and extreme inputs (|x|
+// outside 1e-300..1e300, where the approximation flushes subnormals) take the IEEE division, so their
+// special values are exactly those of 1/x.
 ABL_HD double rcp64(double x) {
 #ifdef __CUDA_ARCH__
     const double ax = fabs(x);
     if (!(ax > 1e-300 && ax < 1e300)) return 1.0 / x;
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    r = r * fma(-x, r, 2.0);
-    r = r * fma(-x, r, 2.0);
+    r = fma(r, fma(-x, r, 1.0), r);
+    r = fma(r, fma(-x, r, 1.0), r);
     return r;
 #else
     return 1.0 / x;
