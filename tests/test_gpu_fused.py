@@ -1,7 +1,7 @@
 """The fused one-pass RHS (k_fused_rhs) against the two-pass kernels and the oracle.
 
-Where a tile's staged rows fit in shared memory the handle runs the fused kernel; ABL_FV_FUSED=0 at
-create keeps the gradient pass + tile flux pass. Both evaluate every gradient and face flux with the
+With ABL_FV_FUSED=1 at create, where a tile's staged rows fit in shared memory, the handle runs the
+fused kernel; otherwise (the default) the gradient pass + tile flux pass. Both evaluate every gradient and face flux with the
 same arithmetic; they differ only in the order a cell sums its face fluxes (the fused kernel sums
 opposite faces next to each other), so they agree to rounding. Both match the oracle at the FP64 bar.
 """
