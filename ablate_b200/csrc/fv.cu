@@ -3,9 +3,11 @@
 // points used by the known-answer tests.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -138,17 +140,27 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
 }
 
 // ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
+// Exact species counts (fv_inst_*.cu, fv_adj_*.cu) and the capacity instances 16 and kMaxSpecies
+// (fv_inst_cap.cu, fv_adj_cap.cu), per dimension, ascending.
+constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSpecies, -1}, {0, 2, 3, 5, 9, 16, kMaxSpecies, -1}};
+
 #define ABL_DISPATCH(fv, FN, ...)                                                                                                  \
     do {                                                                                                                           \
-        switch ((fv)->dim * 100 + (fv)->ns) {                                                                                      \
-            case 100: FN<1, 0>(fv, __VA_ARGS__); break;                                                                            \
-            case 200: FN<2, 0>(fv, __VA_ARGS__); break;                                                                            \
-            case 202: FN<2, 2>(fv, __VA_ARGS__); break;                                                                            \
-            case 203: FN<2, 3>(fv, __VA_ARGS__); break;                                                                            \
-            case 300: FN<3, 0>(fv, __VA_ARGS__); break;                                                                            \
-            case 302: FN<3, 2>(fv, __VA_ARGS__); break;                                                                            \
-            case 305: FN<3, 5>(fv, __VA_ARGS__); break;                                                                            \
-            case 309: FN<3, 9>(fv, __VA_ARGS__); break;                                                                            \
+        switch ((fv)->dim * 1000 + (fv)->ns) {                                                                                     \
+            case 1000: FN<1, 0>(fv, __VA_ARGS__); break;                                                                           \
+            case 1016: FN<1, 16>(fv, __VA_ARGS__); break;                                                                          \
+            case 1000 + kMaxSpecies: FN<1, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
+            case 2000: FN<2, 0>(fv, __VA_ARGS__); break;                                                                           \
+            case 2002: FN<2, 2>(fv, __VA_ARGS__); break;                                                                           \
+            case 2003: FN<2, 3>(fv, __VA_ARGS__); break;                                                                           \
+            case 2016: FN<2, 16>(fv, __VA_ARGS__); break;                                                                          \
+            case 2000 + kMaxSpecies: FN<2, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
+            case 3000: FN<3, 0>(fv, __VA_ARGS__); break;                                                                           \
+            case 3002: FN<3, 2>(fv, __VA_ARGS__); break;                                                                           \
+            case 3005: FN<3, 5>(fv, __VA_ARGS__); break;                                                                           \
+            case 3009: FN<3, 9>(fv, __VA_ARGS__); break;                                                                           \
+            case 3016: FN<3, 16>(fv, __VA_ARGS__); break;                                                                          \
+            case 3000 + kMaxSpecies: FN<3, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
             default: throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for this dimension/species count");          \
         }                                                                                                                          \
     } while (0)
@@ -165,9 +177,76 @@ void dispatch_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cud
     ABL_DISPATCH(fv, run_vjp, U, Fb, Ub, s);
 }
 
-bool rhs_supported(int dim, int ns) {
-    const int key = dim * 100 + ns;
-    return key == 100 || key == 200 || key == 202 || key == 203 || key == 300 || key == 302 || key == 305 || key == 309;
+// The instance that runs ns species in dim dimensions: the smallest compiled one that holds them (-1:
+// none). ABL_FV_SPECIES_INSTANCE, read at create, asks for a larger one (a count then runs padded).
+int instance_for(int dim, int ns) {
+    int want = ns;
+    if (const char* v = std::getenv("ABL_FV_SPECIES_INSTANCE")) want = std::max(ns, std::atoi(v));
+    if (dim < 1 || dim > 3) return -1;
+    for (int i = 0; i < 8 && kInstances[dim - 1][i] >= 0; i++)
+        if (kInstances[dim - 1][i] >= want) return kInstances[dim - 1][i];
+    return -1;
+}
+
+// ---- species padding ----------------------------------------------------------------------------
+// A count without an instance of its own runs in a larger one: its rows there are [euler | pad
+// zero-state species | the caller's species]. Padding species have zero NASA-7 rows, infinite molar
+// mass (1/W = 0, h_ref = 0) and zero diffusivity, so every term they add to a sum is an exact zero;
+// they come first so that the mixture's closing species (TChem's clipping gives the last species
+// 1 - sum of the others) is the caller's last. Their limited gradient is zero (the limiters map the
+// 0/0 ratio of a constant component to a zero factor, as PetscLimiterLimit's min/max forms do), and
+// their own residual rows, zero, are dropped.
+// rows [n][w] -> [n][w + pad], pad zero columns after column ne
+__global__ void __launch_bounds__(256) k_pad_rows(const double* __restrict__ src, int64_t n, int w, int ne, int pad, double* __restrict__ dst) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int wi = w + pad;
+    if (e >= n * wi) return;
+    const int64_t i = e / wi;
+    const int k = (int)(e - i * wi);
+    dst[e] = k < ne ? src[i * w + k] : (k < ne + pad ? 0.0 : src[i * w + k - pad]);
+}
+// back: the listed rows (or all n) of [..][w + pad] into [..][w], the pad columns dropped; added or assigned
+__global__ void __launch_bounds__(256) k_unpad_rows(const double* __restrict__ src, int64_t n, const int* __restrict__ rows, int w, int ne, int pad,
+                                                    double* __restrict__ dst, int add) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n * w) return;
+    const int64_t j = e / w;
+    const int k = (int)(e - j * w);
+    const int64_t r = rows ? (int64_t)__ldg(rows + j) : j;
+    const double v = src[r * (w + pad) + (k < ne ? k : k + pad)];
+    double* d = dst + r * w + k;
+    *d = add ? *d + v : v;
+}
+
+// the caller's state rows in the instance's width (the scratch buffer), or the rows themselves
+const double* pad_in(abl_fv* fv, DevBuf<double>& scratch, const double* user, cudaStream_t s) {
+    if (fv->pad == 0) return user;
+    const size_t n = (size_t)fv->n_cells * fv->nc;
+    if (scratch.n != n) scratch.alloc(n);
+    k_pad_rows<<<blocks_for((long)n, 256), 256, 0, s>>>(user, fv->n_cells, fv->nc_user, 2 + fv->dim, fv->pad, scratch.p);
+    check_launch();
+    return scratch.p;
+}
+// a zeroed residual buffer in the instance's width
+double* pad_out(abl_fv* fv, DevBuf<double>& scratch, cudaStream_t s) {
+    const size_t n = (size_t)fv->n_cells * fv->nc;
+    if (scratch.n != n) scratch.alloc(n);
+    ABL_CUDA(cudaMemsetAsync(scratch.p, 0, n * sizeof(double), s));
+    return scratch.p;
+}
+// rows of the instance's residual into the caller's (owned rows only, or all)
+void unpad_rows(abl_fv* fv, const double* inst, double* user, bool owned_only, bool add, cudaStream_t s) {
+    const int64_t n = owned_only ? (int64_t)fv->owned_rows.n : (int64_t)fv->n_cells;
+    if (n == 0) return;
+    k_unpad_rows<<<blocks_for((long)(n * fv->nc_user), 256), 256, 0, s>>>(inst, n, owned_only ? fv->owned_rows.p : nullptr, fv->nc_user, 2 + fv->dim,
+                                                                           fv->pad, user, add ? 1 : 0);
+    check_launch();
+}
+// entry points that work on the instance's rows directly need a count with an instance of its own
+void require_exact_instance(const abl_fv* fv, const char* what) {
+    if (fv->pad)
+        throw AblError(ABL_ERR_UNSUPPORTED, std::string(what) + ": " + std::to_string(fv->ns_user) +
+                                                " species run padded in a larger instance; this entry point needs a count with an instance of its own");
 }
 
 // ---- batch kernels ------------------------------------------------------------------------------
@@ -350,9 +429,33 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         validate_physics(physics);
         if (!mesh) throw std::invalid_argument("mesh descriptor is NULL");
         if (mesh->dim < 1 || mesh->dim > 3) throw std::invalid_argument("invalid mesh descriptor: dim must be 1, 2 or 3");
-        if (!rhs_supported(mesh->dim, physics->n_species))
+        const int ns_user = physics->n_species;
+        const int ns_inst = instance_for(mesh->dim, ns_user);
+        if (ns_inst < 0)
             throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for dim " + std::to_string(mesh->dim) + " with " +
-                                                    std::to_string(physics->n_species) + " species");
+                                                    std::to_string(ns_user) + " species");
+        // the caller's physics in the instance's species layout (padding species first)
+        const int pad = ns_inst - ns_user;
+        abl_physics_desc padded = *physics;
+        std::vector<double> pnasa7, pmw, pdiff;
+        if (pad > 0) {
+            padded.n_species = ns_inst;
+            if (physics->eos == ABL_EOS_NASA7) {
+                pnasa7.assign(15 * (size_t)pad, 0.0);
+                pnasa7.insert(pnasa7.end(), physics->nasa7, physics->nasa7 + 15 * (size_t)ns_user);
+                pmw.assign((size_t)pad, std::numeric_limits<double>::infinity());
+                pmw.insert(pmw.end(), physics->mw, physics->mw + ns_user);
+                padded.nasa7 = pnasa7.data();
+                padded.mw = pmw.data();
+            }
+            if (physics->species_diff) {
+                pdiff.assign((size_t)pad, 0.0);
+                pdiff.insert(pdiff.end(), physics->species_diff, physics->species_diff + ns_user);
+                padded.species_diff = pdiff.data();
+            }
+            validate_physics(&padded);
+            physics = &padded;
+        }
         const bool lsq = physics->reconstruction == ABL_RECON_LEASTSQUARES;
         const bool dif = (physics->diffusion || (physics->species_diffusion && physics->n_species > 0)) && physics->transport != ABL_TRANSPORT_NONE;
         // the descriptor is checked and set up on the host first, so a corrupt mesh is rejected the same
@@ -370,6 +473,10 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->ns = physics->n_species;
         fv->nc = 2 + h.dim + fv->ns;
         fv->naux = 1 + h.dim + fv->ns;
+        fv->ns_user = ns_user;
+        fv->pad = pad;
+        fv->nc_user = fv->nc - pad;
+        fv->naux_user = fv->naux - pad;
         fv->n_cells = h.n_cells;
         fv->n_faces = h.n_faces;
         fv->n_flux_faces = (int)h.flux_faces.size();
@@ -411,9 +518,17 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             Tiles b = build_tiles(h, mesh, tile, true);
             return b.tf_cells.size() < a.tf_cells.size() ? b : a;
         };
+        // and whose shared memory fits every pass: the face fluxes (value and tangent pairs in the JVP) and
+        // the adjoint's per-cell accumulator rows (state, gradient, aux, aux gradient; odd stride)
+        const int naux_ = 1 + h.dim + physics->n_species;
+        const size_t adj_row = (size_t)((nc_ + nc_ * h.dim + naux_ + naux_ * h.dim) | 1) * sizeof(double);
+        auto fits = [&](const Tiles& t, int cells) {
+            const size_t faces = (size_t)std::max(t.max_faces, 1) * nc_ * sizeof(double);
+            return faces <= 200 * 1024 && 2 * faces <= 227 * 1024 && (size_t)cells * adj_row <= 227 * 1024;
+        };
         int tile = 256;
         Tiles tl = tiles_for(tile);
-        while ((size_t)tl.max_faces * nc_ * sizeof(double) > 200 * 1024 && tile > 16) {
+        while (!fits(tl, tile) && tile > 16) {
             tile /= 2;
             tl = tiles_for(tile);
         }
@@ -695,8 +810,8 @@ int abl_fv_profile_read(abl_fv* fv, int32_t* n, float* ms, char* names) {
 
 int abl_fv_sizes(const abl_fv* fv, int32_t* nc, int32_t* naux, int32_t* n_cells, int32_t* n_faces) {
     if (!fv) return fail(ABL_ERR_INVALID_ARGUMENT, "handle is NULL");
-    if (nc) *nc = fv->nc;
-    if (naux) *naux = fv->naux;
+    if (nc) *nc = fv->nc_user;
+    if (naux) *naux = fv->naux_user;
     if (n_cells) *n_cells = fv->n_cells;
     if (n_faces) *n_faces = fv->n_faces;
     return ABL_OK;
@@ -726,7 +841,16 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
         precision &= ~ABL_RHS_OVERWRITE;
         if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
         ABL_CUDA(cudaSetDevice(fv->device));
-        dispatch_rhs(fv, U_dev, F_dev, precision, overwrite, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (fv->pad == 0) {
+            dispatch_rhs(fv, U_dev, F_dev, precision, overwrite, s);
+            return;
+        }
+        // a padded count: the instance's rows in scratch, the residual back into the caller's rows
+        const double* U = pad_in(fv, fv->pU, U_dev, s);
+        double* F = pad_out(fv, fv->pF, s);
+        dispatch_rhs(fv, U, F, precision, 1, s);
+        unpad_rows(fv, F, F_dev, true, !overwrite, s);
     });
 }
 
@@ -738,7 +862,18 @@ int abl_fv_jvp(abl_fv* fv, double time, const double* U_dev, const double* dU_de
         // value + tangent gradient pairs, allocated on first use
         if (fv->need_state_grad && fv->gradD.n == 0) fv->gradD.alloc((size_t)fv->n_cells * fv->nc * fv->dim * 2);
         if (fv->need_aux_grad && fv->agradD.n == 0) fv->agradD.alloc((size_t)fv->n_cells * fv->naux * fv->dim * 2);
-        dispatch_jvp(fv, U_dev, dU_dev, F_dev, dF_dev, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (fv->pad == 0) {
+            dispatch_jvp(fv, U_dev, dU_dev, F_dev, dF_dev, s);
+            return;
+        }
+        const double* U = pad_in(fv, fv->pU, U_dev, s);
+        const double* dU = pad_in(fv, fv->pdU, dU_dev, s);
+        double* F = F_dev ? pad_out(fv, fv->pF, s) : nullptr;
+        double* dF = pad_out(fv, fv->pdF, s);
+        dispatch_jvp(fv, U, dU, F, dF, s);
+        if (F_dev) unpad_rows(fv, F, F_dev, true, true, s);
+        unpad_rows(fv, dF, dF_dev, true, true, s);
     });
 }
 
@@ -746,7 +881,7 @@ int abl_fv_jvp_host(abl_fv* fv, double time, const double* U_host, const double*
     return guarded([&] {
         if (!fv || !U_host || !dU_host || !dF_host) throw std::invalid_argument("abl_fv_jvp_host: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        const size_t n = (size_t)fv->n_cells * fv->nc;
+        const size_t n = (size_t)fv->n_cells * fv->nc_user;
         if (fv->hU.n != n) fv->hU.alloc(n);
         if (fv->hdU.n != n) fv->hdU.alloc(n);
         if (fv->hdF.n != n) fv->hdF.alloc(n);
@@ -783,7 +918,17 @@ int abl_fv_vjp(abl_fv* fv, double time, const double* U_dev, const double* Fbar_
                 fv->adj_ist.alloc(n * fv->nc);
             }
         }
-        dispatch_vjp(fv, U_dev, Fbar_dev, Ubar_dev, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (fv->pad == 0) {
+            dispatch_vjp(fv, U_dev, Fbar_dev, Ubar_dev, s);
+            return;
+        }
+        // every cell's adjoint row (boundary ghosts and halos included) goes back to the caller
+        const double* U = pad_in(fv, fv->pU, U_dev, s);
+        const double* Fb = pad_in(fv, fv->pF, Fbar_dev, s);
+        double* Ub = pad_out(fv, fv->pUb, s);
+        dispatch_vjp(fv, U, Fb, Ub, s);
+        unpad_rows(fv, Ub, Ubar_dev, false, true, s);
     });
 }
 
@@ -791,7 +936,7 @@ int abl_fv_vjp_host(abl_fv* fv, double time, const double* U_host, const double*
     return guarded([&] {
         if (!fv || !U_host || !Fbar_host || !Ubar_host) throw std::invalid_argument("abl_fv_vjp_host: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        const size_t n = (size_t)fv->n_cells * fv->nc;
+        const size_t n = (size_t)fv->n_cells * fv->nc_user;
         if (fv->hU.n != n) fv->hU.alloc(n);
         if (fv->hdU.n != n) fv->hdU.alloc(n);
         if (fv->hdF.n != n) fv->hdF.alloc(n);
@@ -808,7 +953,9 @@ int abl_fv_update_aux(abl_fv* fv, const double* U_dev, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_update_aux: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_DISPATCH(fv, run_aux, U_dev, static_cast<cudaStream_t>(stream));
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const double* U = pad_in(fv, fv->pU, U_dev, s);
+        ABL_DISPATCH(fv, run_aux, U, s);
     });
 }
 
@@ -816,7 +963,7 @@ int abl_fv_update_aux_host(abl_fv* fv, const double* U_host) {
     return guarded([&] {
         if (!fv || !U_host) throw std::invalid_argument("abl_fv_update_aux_host: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        const size_t n = (size_t)fv->n_cells * fv->nc;
+        const size_t n = (size_t)fv->n_cells * fv->nc_user;
         if (fv->hU.n != n) fv->hU.alloc(n);
         ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
         int rc = abl_fv_update_aux(fv, fv->hU.p, nullptr);
@@ -833,9 +980,18 @@ int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_hos
     return guarded([&] {
         if (!fv || !U_host || !F_host) throw std::invalid_argument("abl_fv_rhs_host: NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        const size_t n = (size_t)fv->n_cells * fv->nc;
+        const size_t n = (size_t)fv->n_cells * fv->nc_user;
         if (fv->hU.n != n) fv->hU.alloc(n);
         if (fv->hF.n != n) fv->hF.alloc(n);
+        if (fv->pad) {
+            // a padded count: plain copies around the device call (no chunked overlap)
+            ABL_CUDA(cudaMemcpy(fv->hU.p, U_host, n * sizeof(double), cudaMemcpyHostToDevice));
+            ABL_CUDA(cudaMemcpy(fv->hF.p, F_host, n * sizeof(double), cudaMemcpyHostToDevice));
+            int rc = abl_fv_rhs(fv, time, fv->hU.p, fv->hF.p, precision & ~ABL_RHS_OVERWRITE, nullptr);
+            if (rc != ABL_OK) throw AblError(rc, g_last_error);
+            ABL_CUDA(cudaMemcpy(F_host, fv->hF.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+            return;
+        }
         if (!fv->host_stream) {
             ABL_CUDA(cudaStreamCreateWithFlags(&fv->host_stream, cudaStreamNonBlocking));
             ABL_CUDA(cudaStreamCreateWithFlags(&fv->copy_stream, cudaStreamNonBlocking));
@@ -887,7 +1043,16 @@ int abl_fv_get_aux(abl_fv* fv, double* aux_host) {
     return guarded([&] {
         if (!fv || !aux_host) throw std::invalid_argument("NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_CUDA(cudaMemcpy(aux_host, fv->aux.p, fv->aux.n * sizeof(double), cudaMemcpyDeviceToHost));
+        if (fv->pad == 0) {
+            ABL_CUDA(cudaMemcpy(aux_host, fv->aux.p, fv->aux.n * sizeof(double), cudaMemcpyDeviceToHost));
+            return;
+        }
+        // rows [T, u | pad | Y] of the instance into the caller's [T, u | Y]
+        std::vector<double> a(fv->aux.n);
+        ABL_CUDA(cudaMemcpy(a.data(), fv->aux.p, a.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        const int ne = 1 + fv->dim;
+        for (size_t c = 0; c < (size_t)fv->n_cells; c++)
+            for (int k = 0; k < fv->naux_user; k++) aux_host[c * fv->naux_user + k] = a[c * fv->naux + (k < ne ? k : k + fv->pad)];
     });
 }
 
@@ -895,7 +1060,15 @@ int abl_fv_set_aux(abl_fv* fv, const double* aux_host) {
     return guarded([&] {
         if (!fv || !aux_host) throw std::invalid_argument("NULL argument");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_CUDA(cudaMemcpy(fv->aux.p, aux_host, fv->aux.n * sizeof(double), cudaMemcpyHostToDevice));
+        if (fv->pad == 0) {
+            ABL_CUDA(cudaMemcpy(fv->aux.p, aux_host, fv->aux.n * sizeof(double), cudaMemcpyHostToDevice));
+            return;
+        }
+        std::vector<double> a(fv->aux.n, 0.0);
+        const int ne = 1 + fv->dim;
+        for (size_t c = 0; c < (size_t)fv->n_cells; c++)
+            for (int k = 0; k < fv->naux_user; k++) a[c * fv->naux + (k < ne ? k : k + fv->pad)] = aux_host[c * fv->naux_user + k];
+        ABL_CUDA(cudaMemcpy(fv->aux.p, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice));
     });
 }
 
@@ -920,6 +1093,7 @@ int abl_fv_launch_count(const abl_fv* fv, int precision, int32_t* launches) {
     const bool fused = fv->fused_ok[precision == ABL_PRECISION_MIXED && fv->ns == 0 ? 1 : 0];
     if (!fused && (fv->need_state_grad || fv->need_aux_grad)) n++;
     if (fv->mesh.n_tiles > 0) n++;
+    if (fv->pad) n += 2;  // rows into the instance's width and back
     *launches = n;
     return ABL_OK;
 }
@@ -1055,6 +1229,7 @@ int abl_eos_batch_noalloc(const abl_physics_desc* physics, int dim, int property
 int abl_fv_set_boundary(abl_fv* fv, int32_t n_bc, const abl_bc* table, const int32_t* cell_bc) {
     return guarded([&] {
         if (!fv || !table || n_bc < 1) throw std::invalid_argument("abl_fv_set_boundary: need a handle and at least one condition");
+        require_exact_instance(fv, "abl_fv_set_boundary");
         for (int b = 0; b < n_bc; b++)
             if (table[b].kind < ABL_BC_OUTFLOW || table[b].kind > ABL_BC_NOSLIP_WALL)
                 throw std::invalid_argument("abl_fv_set_boundary: unknown condition kind in entry " + std::to_string(b));
@@ -1139,6 +1314,7 @@ int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream) {
     (void)time;
     return guarded([&] {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_fill_ghosts: NULL argument");
+        require_exact_instance(fv, "abl_fv_fill_ghosts");
         ABL_CUDA(cudaSetDevice(fv->device));
         ABL_DISPATCH(fv, run_fill_ghosts, U_dev, static_cast<cudaStream_t>(stream));
     });
@@ -1155,6 +1331,7 @@ int abl_fv_set_jvp_mode(abl_fv* fv, int mode) {
 int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream) {
     return guarded([&] {
         if (!fv || !dU_dev) throw std::invalid_argument("abl_fv_fill_ghosts_jvp: NULL argument");
+        require_exact_instance(fv, "abl_fv_fill_ghosts_jvp");
         ABL_CUDA(cudaSetDevice(fv->device));
         ABL_DISPATCH(fv, run_fill_ghosts_jvp, dU_dev, static_cast<cudaStream_t>(stream));
     });
@@ -1163,6 +1340,7 @@ int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream) {
 int abl_fv_fill_ghosts_vjp(abl_fv* fv, double* Ubar_dev, double* value_bar_host, void* stream) {
     return guarded([&] {
         if (!fv || !Ubar_dev) throw std::invalid_argument("abl_fv_fill_ghosts_vjp: NULL argument");
+        require_exact_instance(fv, "abl_fv_fill_ghosts_vjp");
         ABL_CUDA(cudaSetDevice(fv->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const size_t nv = (size_t)fv->n_bc * ABL_BC_MAX_COMPONENTS;
@@ -1181,6 +1359,7 @@ int abl_fv_fill_ghosts_vjp(abl_fv* fv, double* Ubar_dev, double* value_bar_host,
 int abl_fv_set_pressure_functional(abl_fv* fv, int32_t n, const int32_t* cells, const double* weights) {
     return guarded([&] {
         if (!fv || n < 0 || (n > 0 && (!cells || !weights))) throw std::invalid_argument("abl_fv_set_pressure_functional: bad argument");
+        require_exact_instance(fv, "abl_fv_set_pressure_functional");
         std::vector<uint8_t> seen(fv->n_cells, 0);
         for (int j = 0; j < n; j++) {
             if (cells[j] < 0 || cells[j] >= fv->n_cells)
@@ -1199,6 +1378,7 @@ int abl_fv_set_pressure_functional(abl_fv* fv, int32_t n, const int32_t* cells, 
 int abl_fv_pressure_functional(abl_fv* fv, const double* U_dev, double* J_host, double* Ubar_dev, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev || !J_host) throw std::invalid_argument("abl_fv_pressure_functional: NULL argument");
+        require_exact_instance(fv, "abl_fv_pressure_functional");
         ABL_CUDA(cudaSetDevice(fv->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         *J_host = 0.0;
@@ -1216,6 +1396,7 @@ int abl_fv_pressure_functional(abl_fv* fv, const double* U_dev, double* J_host, 
 int abl_fv_cfl_dt(abl_fv* fv, const double* U_dev, double cfl, double* dt_host, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev || !dt_host) throw std::invalid_argument("abl_fv_cfl_dt: NULL argument");
+        require_exact_instance(fv, "abl_fv_cfl_dt");
         if (!(cfl > 0)) throw std::invalid_argument("abl_fv_cfl_dt: cfl must be positive");
         ABL_CUDA(cudaSetDevice(fv->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1230,6 +1411,7 @@ int abl_fv_cfl_dt(abl_fv* fv, const double* U_dev, double cfl, double* dt_host, 
 int abl_fv_normalize_species(abl_fv* fv, double* U_dev, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_normalize_species: NULL argument");
+        require_exact_instance(fv, "abl_fv_normalize_species");
         ABL_CUDA(cudaSetDevice(fv->device));
         ABL_DISPATCH(fv, run_normalize, U_dev, static_cast<cudaStream_t>(stream));
     });
@@ -1239,6 +1421,7 @@ int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const 
                     void* stream) {
     return guarded([&] {
         if (!fv || !Us_dev || !F_dev || !Uout_dev || (a != 0.0 && !U0_dev)) throw std::invalid_argument("abl_fv_rk_stage: NULL argument");
+        require_exact_instance(fv, "abl_fv_rk_stage");
         ABL_CUDA(cudaSetDevice(fv->device));
         rk_stage(fv, a, U0_dev, b, Us_dev, dt, F_dev, Uout_dev, static_cast<cudaStream_t>(stream));
     });
@@ -1247,6 +1430,7 @@ int abl_fv_rk_stage(abl_fv* fv, double a, const double* U0_dev, double b, const 
 int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, int precision, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_step: NULL argument");
+        require_exact_instance(fv, "abl_fv_step");
         if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
         if (scheme != ABL_STEP_EULER && scheme != ABL_STEP_SSPRK3) throw std::invalid_argument("abl_fv_step: unknown scheme");
         ABL_CUDA(cudaSetDevice(fv->device));
@@ -1312,6 +1496,7 @@ int abl_fv_upload_owned(abl_fv* fv, const double* host, int width, double* dst_d
 int abl_fv_step_cfl(abl_fv* fv, int scheme, double cfl, double* U_dev, int precision, double* time_dev, void* stream) {
     return guarded([&] {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_step_cfl: NULL argument");
+        require_exact_instance(fv, "abl_fv_step_cfl");
         if (!(cfl > 0)) throw std::invalid_argument("abl_fv_step_cfl: cfl must be positive");
         if (precision != ABL_PRECISION_FP64 && precision != ABL_PRECISION_MIXED) throw std::invalid_argument("unknown precision");
         if (scheme != ABL_STEP_EULER && scheme != ABL_STEP_SSPRK3) throw std::invalid_argument("abl_fv_step_cfl: unknown scheme");

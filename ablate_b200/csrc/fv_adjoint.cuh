@@ -61,7 +61,7 @@ ABL_HD void fill_y_vjp(int ns, double rho, const double* rhoY, const double* ysb
     double y[NSMAX > 0 ? NSMAX : 1];
     bool act[NSMAX > 0 ? NSMAX : 1];
     double sum = 0.0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < ns - 1; s++) {
         const double raw = rhoY[s] * irho;
         act[s] = raw > 0.0 && !(1.0 < raw);
@@ -70,10 +70,10 @@ ABL_HD void fill_y_vjp(int ns, double rho, const double* rhoY, const double* ysb
     }
     double irhob = 0.0, dot = 0.0;
     if (sum > 1.0) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int s = 0; s < ns - 1; s++) dot += ysb[s] * y[s];
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < ns - 1; s++) {
         double yb = sum > 1.0 ? ysb[s] / sum - dot / (sum * sum) : ysb[s] - ysb[ns - 1];
         if (!act[s]) yb = 0.0;
@@ -87,10 +87,10 @@ ABL_HD void fill_y_vjp(int ns, double rho, const double* rhoY, const double* ysb
 template <int DIM, int NSMAX>
 ABL_HD void nasa_temperature_vjp(const Phys& P, int ns, const double* U, const double* ys, double T, double Tb, double* ysb, double* Ub) {
     double cv = 0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < ns; k++) cv += ys[k] * (nasa_cp_molar(P.nasa7 + 15 * k, T) - kRuniv) * P.inv_mw[k];
     const double q = Tb / cv;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < ns; k++)
         ysb[k] -= q * (nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k]);
     internal_energy_vjp<DIM>(U, q, Ub);
@@ -113,7 +113,7 @@ ABL_HD void decode_vjp(const Phys& P, int ns, const double* U, const Decoded<dou
     fill_y(ns, rho, U + 2 + DIM, ys);
     const double T = dd.T;
     double cp = 0, iw = 0, dcp = 0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < ns; k++) {
         cp += ys[k] * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
         dcp += ys[k] * nasa_dcp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
@@ -132,7 +132,7 @@ ABL_HD void decode_vjp(const Phys& P, int ns, const double* U, const Decoded<dou
     Rb += gb * cp / (cv * cv);
     Tb += cpb * dcp;
     // e = e_s(T, Y): de/dT = cv, de/dY_k = e_s,k
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < ns; k++) {
         const double esk = nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k];
         ysb[k] += eb * esk + cpb * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] + Rb * kRuniv * P.inv_mw[k];
@@ -150,7 +150,7 @@ ABL_HD void cp_at_vjp(const Phys& P, int ns, const double* U, double T, double c
     double ys[NY], ysb[NY];
     fill_y(ns, U[0], U + 2 + DIM, ys);
     double dcp = 0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < ns; k++) {
         dcp += ys[k] * nasa_dcp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
         ysb[k] = cpb * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
@@ -198,7 +198,7 @@ __device__ __forceinline__ void cell_aux_vjp(const Phys& P, const double* u, con
         Ub[2 + d] += ab[1 + d] * irho;
         irhob += ab[1 + d] * u[2 + d];
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < NS; s++) {
         Ub[D::NE + s] += ab[1 + DIM + s] * irho;
         irhob += ab[1 + DIM + s] * u[D::NE + s];
@@ -211,7 +211,7 @@ __device__ __forceinline__ void cell_aux_vjp(const Phys& P, const double* u, con
         fill_y(NS, u[0], u + D::NE, ys);
         bool ok = true;
         const double T = temperature<DIM, NS>(P, NS, u, __ldg(aux + (size_t)c * D::NA), &ok);
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < NS; k++) ysb[k] = 0.0;
         nasa_temperature_vjp<DIM, NS>(P, NS, u, ys, T, ab[0], ysb, Ub);
         fill_y_vjp<NS>(NS, u[0], u + D::NE, ysb, Ub, Ub + D::NE);
@@ -517,7 +517,7 @@ __device__ __forceinline__ void advection_vjp_side(const Phys& P, unsigned mask,
     if (NS > 0 && spadv && dir == ABL_DIR_NA && P.sp_compact) {
         // compact process, no direction: flux_s = mA (rhoY_L + rhoY_R) / (rho_L + rho_R) (both halves)
         const double rhoM = 0.5 * (rho + rho_o), irm = 1.0 / rhoM;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int s = 0; s < NS; s++) {
             const double ry = u[D::NE + s], ry_o = xch(mask, ry);
             const double num = 0.5 * (side ? ry + ry_o : ry_o + ry);
@@ -526,7 +526,7 @@ __device__ __forceinline__ void advection_vjp_side(const Phys& P, unsigned mask,
             ub[0] -= 0.5 * mA * num * irm * irm * fb[D::NE + s];
         }
     } else if (NS > 0 && spadv) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int s = 0; s < NS; s++) {
             const double Y = u[D::NE + s] * irho;
             const double Y_o = xch(mask, Y);
@@ -559,11 +559,11 @@ template <int DIM, int NS>
 __device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* normal, const double* fs, const double* fa, const double* gf, bool dif,
                                               bool spdif, const double* fb, double* fsb, double* fab, double* gfb) {
     using D = Dims<DIM, NS>;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) fsb[k] = 0.0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA; k++) fab[k] = 0.0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA * DIM; k++) gfb[k] = 0.0;
     double mu, kc, diff;
     transport<DIM, NS>(P, NS, fs, fa[0], &mu, &kc, &diff);
@@ -617,7 +617,7 @@ __device__ __forceinline__ void diffusion_vjp(const Phys& P, const double* norma
             const double density = fs[0];
             const int yoff = (1 + DIM) * DIM;
             double rhob = 0, Tb = 0;
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int s = 0; s < NS; ++s) {
                 const double hs = P.eos == ABL_EOS_NASA7 ? nasa_h_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s] - P.href[s] : 0.0;
                 // one constant D_k per species (no state dependence), or the transport model's D
@@ -665,7 +665,7 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
     const bool own = M.kind[me] == ABL_CELL_OWNED;
     const double iv = own ? M.ivol[me] : 0.0;
     double fb[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         const double t = own ? __ldg(Fb + (size_t)me * D::NC + k) * iv : 0.0;
         const double mine = side ? t : -t;
@@ -678,7 +678,7 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
     if (adv || spadv) {
         const bool lsq = P.recon == ABL_RECON_LEASTSQUARES;
         double u[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             double dot = 0;
             if (lsq) {
@@ -694,12 +694,12 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
             guess = side ? TL * .33 + .67 * TR : TL * .67 + .33 * TR;
         }
         double ub[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) ub[k] = 0.0;
         advection_vjp_side<DIM, NS, FK>(P, mask, side, normal, u, guess, adv, spadv, fb, ub, ok, rok);
         // u_face = u_cell + g . dx: the identity part to the state, the outer product with dx to the gradient
         if (dst) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) {
                 dst[AR::U + k] += ub[k];
                 if (lsq)
@@ -716,10 +716,10 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
         {
             double a[D::NA];
             cell_aux<DIM, NS>(P, c, aux, me, a);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) fa[k] = a[k] * 0.5 + xch(mask, a[k]) * 0.5;
         }
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) fs[k] = c[k] * 0.5 + xch(mask, c[k]) * 0.5;
         // the face gradient: in 1D the two-cell LeastSquares stencil's (w_L a_L + w_R a_R, the same sum
         // in both lanes), else the average of the two cells' aux gradients
@@ -733,13 +733,13 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
             const double wot = side ? wl : wr;
             double a[D::NA];
             cell_aux<DIM, NS>(P, c, aux, me, a);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) {
                 const double mine = a[k] * wme, other = xch(mask, a[k]) * wot;
                 gf[k] = side ? other + mine : mine + other;
             }
         } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA * DIM; k++) {
                 const double gm = __ldg(agrad + (size_t)me * GR::AS + k);
                 gf[k] = 0.5 * gm + 0.5 * xch(mask, gm);
@@ -748,15 +748,15 @@ __device__ __forceinline__ void face_vjp_side(const DevMesh& M, const Phys& P, u
         double fsb[D::NC], fab[D::NA], gfb[D::NA * DIM];
         diffusion_vjp<DIM, NS>(P, normal, fs, fa, gf, dif, spdif, fb, fsb, fab, gfb);
         if (dst) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) dst[AR::U + k] += 0.5 * fsb[k];
             if constexpr (DIM == 1) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k] + wme * gfb[k];
             } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NA; k++) dst[AR::A + k] += 0.5 * fab[k];
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NA * DIM; k++) dst[AR::GA + k] += 0.5 * gfb[k];
             }
         }
@@ -793,19 +793,19 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
     const uint8_t kind = M.kind[c];
     double ub[D::NC], gbar[D::NC * DIM], beta[D::NC];
     int fst[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         ub[k] = acc[AR::U + k];
         beta[k] = 0.0;
         fst[k] = -1;
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC * DIM; k++) gbar[k] = 0.0;
     if (do_state && (kind == ABL_CELL_OWNED || kind == ABL_CELL_HALO)) {
         // g~ = phi g (0 when cancelled): g-bar = phi g~-bar, plus the limiter's own dependence on g and on
         // the minimising neighbour through r = (u_n - u_c) / (2 g . dx)
         const double* g = rec.graw + (size_t)c * GR::GS;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             const double ph = __ldg(rec.phi + (size_t)c * D::NC + k);
             const int i = __ldg(rec.ist + (size_t)c * D::NC + k);
@@ -841,30 +841,30 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
             const double ws = __ldg(M.wsum + 6 * (size_t)c + d);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) ub[k] -= ws * gbar[k * DIM + d];
         }
     }
     double ab[D::NA], gab[D::NA * DIM];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA; k++) ab[k] = acc[AR::A + k];
     const bool auxg = do_aux && kind != ABL_CELL_HALO_OUTER;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA * DIM; k++) gab[k] = auxg ? acc[AR::GA + k] : 0.0;
     if (auxg) {
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
             const double ws = __ldg(M.wsum + 6 * (size_t)c + 3 + d);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) ab[k] -= ws * gab[k * DIM + d];
         }
     }
     if (out.gb) {
         double* o = out.gb + (size_t)c * GR::GS;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC * DIM; k++) o[k] = gbar[k];
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         out.beta[(size_t)c * D::NC + k] = beta[k];
         out.fstar[(size_t)c * D::NC + k] = fst[k];
@@ -872,10 +872,10 @@ __device__ __forceinline__ void cell_vjp(const DevMesh& M, const Phys& P, int c,
     }
     if (out.gab) {
         double* o = out.gab + (size_t)c * GR::AS;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NA * DIM; k++) o[k] = gab[k];
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA; k++) out.ab[(size_t)c * D::NA + k] = ab[k];
 }
 
@@ -946,13 +946,13 @@ __global__ void __launch_bounds__(128) k_adjoint_nonowned(DevMesh M, Phys P, con
     if (j >= M.n_nonowned) return;
     const int c = M.nonowned[j];
     double acc[AR::N];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < AR::N; k++) acc[k] = 0.0;
     for (int i = M.cone_ptr[c]; i < M.cone_ptr[c + 1]; i++) {
         const int nb = M.face_nb[M.cone[i].x];
         if (nb < 0) continue;
         const double* r = nbrec + (size_t)nb * AR::N;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < AR::N; k++) acc[k] += r[k];
     }
     cell_vjp<DIM, NS, LIM>(M, P, c, U, acc, rec, out, do_state, do_aux);
@@ -966,9 +966,9 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M.n_cells) return;
     double ub[D::NC], ab[D::NA];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) ub[k] = in.ub[(size_t)m * D::NC + k];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA; k++) ab[k] = in.ab[(size_t)m * D::NA + k];
     const int beg = M.cone_ptr[m];
     const size_t wb = weight_base(M, m, beg);
@@ -982,19 +982,19 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
             if (!(ce.y & kConeBoundary)) {
                 double gn[D::NC * DIM];
                 load_row<D::NC * DIM, double>(in.gb + (size_t)n * GR::GS, gn);
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++)
 #pragma unroll
                     for (int d = 0; d < DIM; d++) ub[k] += w[d] * gn[k * DIM + d];
             }
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++)
                 if (__ldg(in.fstar + (size_t)n * D::NC + k) == f) ub[k] += __ldg(in.beta + (size_t)n * D::NC + k);
         }
         if (do_aux) {
             double gn[D::NA * DIM];
             load_row<D::NA * DIM, double>(in.gab + (size_t)n * GR::AS, gn);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++)
 #pragma unroll
                 for (int d = 0; d < DIM; d++) ab[k] += wa[d] * gn[k * DIM + d];
@@ -1004,7 +1004,7 @@ __global__ void __launch_bounds__(128) k_adjoint_gather(DevMesh M, Phys P, const
     load_state<DIM, NS>(U, m, u);
     cell_aux_vjp<DIM, NS>(P, u, aux, m, ab, ub);
     bool finite = true;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         Ub[(size_t)m * D::NC + k] += ub[k];
         finite = finite && isfinite(ub[k]);

@@ -59,14 +59,14 @@ struct SharedRows {
     bool nasa;
     template <class S>
     __device__ __forceinline__ void state(int c, S* u) const {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) u[k] = sU[(size_t)c * D::NC + k];
     }
     __device__ __forceinline__ double temperature(int c) const { return sA[(size_t)c * D::NA]; }
     template <class S>
     __device__ __forceinline__ void aux_of(const Phys& P, const S* u, int c, S* a) const {
         if (NS > 0 && nasa) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) a[k] = sA[(size_t)c * D::NA + k];
         } else {
             aux_from_state<DIM, NS>(P, u, a);
@@ -75,7 +75,7 @@ struct SharedRows {
     template <int N>
     __device__ __forceinline__ void row(const G* p, G* out) const {
         if constexpr (sizeof(G) == 8) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int i = 0; i < N / 2; i++) {
                 const double2 v = reinterpret_cast<const double2*>(p)[i];
                 out[2 * i] = v.x;
@@ -83,7 +83,7 @@ struct SharedRows {
             }
             if constexpr (N % 2) out[N - 1] = p[N - 1];
         } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int i = 0; i < N / 4; i++) {
                 const float4 v = reinterpret_cast<const float4*>(p)[i];
                 out[4 * i] = v.x;
@@ -91,7 +91,7 @@ struct SharedRows {
                 out[4 * i + 2] = v.z;
                 out[4 * i + 3] = v.w;
             }
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int i = (N / 4) * 4; i < N; i++) out[i] = p[i];
         }
     }
@@ -106,7 +106,7 @@ __device__ __forceinline__ void limit_field_shared(const DevMesh& M, const Phys&
                                                    size_t wb, const double* uc, G* g, int k0, int k1) {
     using D = Dims<DIM, NS>;
     G phi[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) phi[k] = big_value<G>();
 #pragma unroll 1
     for (int i = beg; i < end; i++) {
@@ -114,7 +114,7 @@ __device__ __forceinline__ void limit_field_shared(const DevMesh& M, const Phys&
 #pragma unroll
         for (int d = 0; d < DIM; d++) v[d] = geo<G>(M.cv, M.cv32, 3 * (wb + (size_t)(i - beg)) + d);
         const double* un = sU + (size_t)(__ldg(nbr + i) & 0xffff) * D::NC;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             if (k < k0 || k >= k1) continue;
             G denom = 0;
@@ -126,7 +126,7 @@ __device__ __forceinline__ void limit_field_shared(const DevMesh& M, const Phys&
         }
     }
     bool cancel = false;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         if (k < k0 || k >= k1) continue;
         if (phi[k] == G(0)) {
@@ -135,7 +135,7 @@ __device__ __forceinline__ void limit_field_shared(const DevMesh& M, const Phys&
                 if (dabs(g[k * DIM + d]) > G(P.max_lim_grad)) cancel = true;
         }
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         if (k < k0 || k >= k1) continue;
 #pragma unroll
@@ -157,9 +157,9 @@ __device__ __forceinline__ void fused_gradient(const DevMesh& M, const Phys& P, 
     src.state(j, uc);
     if (auxg) src.aux_of(P, uc, j, ac);
     G g[D::NC * DIM], ga[D::NA * DIM];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC * DIM; k++) g[k] = G(0);
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA * DIM; k++) ga[k] = G(0);
     if (state || auxg) {
 #pragma unroll 1
@@ -171,7 +171,7 @@ __device__ __forceinline__ void fused_gradient(const DevMesh& M, const Phys& P, 
             G wd[DIM], wad[DIM];
             cone_weights<DIM, G>(M.cwa, M.cwa32, wb + (size_t)(i - beg), wd, wad);
             if (state && !(nb >> 16)) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) {
                     const G delta = G(un[k] - uc[k]);
 #pragma unroll
@@ -181,7 +181,7 @@ __device__ __forceinline__ void fused_gradient(const DevMesh& M, const Phys& P, 
             if (auxg) {
                 double an[D::NA];
                 src.aux_of(P, un, n, an);
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NA; k++) {
                     const G delta = G(an[k] - ac[k]);
 #pragma unroll
@@ -195,11 +195,11 @@ __device__ __forceinline__ void fused_gradient(const DevMesh& M, const Phys& P, 
         }
     }
     if (do_state) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC * DIM; k++) out[k] = g[k];
     }
     if (do_aux) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NA * DIM; k++) out[GR::GS + k] = ga[k];
     }
 }
@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             double flux[D::NC];
             face_flux<DIM, NS, G, FK>(P, src, lr & 0xffff, (int)((unsigned)lr >> 16), normal, fdx, flux, &ok, &rok);
             double* out = sF + (size_t)i * D::NC;
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) out[k] = flux[k];
         }
         __syncthreads();
@@ -278,22 +278,22 @@ __global__ void __launch_bounds__(kFusedThreads, 1)
             const double iv = __ldg(M.ivol + c);
             // the signed face fluxes summed first, then scaled by 1/V once (as k_tile_flux)
             double sum[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) sum[k] = 0.0;
             const int e0 = __ldg(tcp + j), e1 = __ldg(tcp + j + 1);
             for (int e = e0; e < e1; e++) {
                 const int code = __ldg(tce + e);
                 const double* ff = sF + (size_t)(code & 0x7fff) * D::NC;
                 if (code & 0x8000) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int k = 0; k < D::NC; k++) sum[k] += ff[k];
                 } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int k = 0; k < D::NC; k++) sum[k] -= ff[k];
                 }
             }
             double* Fc = F + (size_t)c * D::NC;
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) {
                 const double acc = (overwrite ? 0.0 : Fc[k]) + sum[k] * iv;
                 Fc[k] = acc;

@@ -70,7 +70,11 @@ inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 struct abl_fv {
     int device = 0;
-    int dim = 0, ns = 0, nc = 0, naux = 0;
+    int dim = 0, ns = 0, nc = 0, naux = 0;  // of the compiled instance that runs (species capacity)
+    // the caller's species count and row widths; pad = ns - ns_user zero-state species sit in front of
+    // the caller's species in the instance's rows (0: the count has an instance of its own)
+    int ns_user = 0, nc_user = 0, naux_user = 0, pad = 0;
+    abl::DevBuf<double> pU, pdU, pF, pdF, pUb;  // rows in the instance's width when pad > 0
     int n_cells = 0, n_faces = 0, n_flux_faces = 0;
     abl::Phys phys{};
     abl::DevMesh mesh{};

@@ -156,13 +156,13 @@ constexpr int kConeNbr = (1 << 30) - 1;
 template <int N, class G>
 __device__ __forceinline__ void load_row(const G* __restrict__ p, G* out) {
     if constexpr (std::is_same<G, Dual>::value) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int i = 0; i < N; i++) {
             const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
             out[i] = Dual(v.x, v.y);
         }
     } else if constexpr (sizeof(G) == 8) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int i = 0; i < N / 2; i++) {
             const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
             out[2 * i] = v.x;
@@ -170,7 +170,7 @@ __device__ __forceinline__ void load_row(const G* __restrict__ p, G* out) {
         }
         if constexpr (N % 2) out[N - 1] = __ldg(p + N - 1);
     } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int i = 0; i < N / 4; i++) {
             const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
             out[4 * i] = v.x;
@@ -178,7 +178,7 @@ __device__ __forceinline__ void load_row(const G* __restrict__ p, G* out) {
             out[4 * i + 2] = v.z;
             out[4 * i + 3] = v.w;
         }
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int i = (N / 4) * 4; i < N; i++) out[i] = __ldg(p + i);
     }
 }
@@ -210,7 +210,7 @@ __device__ __forceinline__ double to_state<double, Dual>(Dual x) {
 template <int DIM, int NS, class S>
 __device__ __forceinline__ void load_state(const double* __restrict__ U, const double* __restrict__ dU, int c, S* u) {
     using D = Dims<DIM, NS>;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         if constexpr (std::is_same<S, Dual>::value)
             u[k] = Dual(__ldg(U + (size_t)c * D::NC + k), __ldg(dU + (size_t)c * D::NC + k));
@@ -235,7 +235,7 @@ __device__ __forceinline__ void aux_from_state(const Phys& P, const S* u, S* a) 
         ke += a[1 + d] * a[1 + d];
     }
     a[0] = (u[1] * irho - 0.5 * ke) * rcp64(P.r_gas / (P.gamma - 1.0));
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
 }
 
@@ -253,10 +253,10 @@ __device__ __forceinline__ void cell_aux(const Phys& P, const S* u, const double
             const S irho = rcp64(u[0]);
 #pragma unroll
             for (int d = 0; d < DIM; d++) a[1 + d] = u[2 + d] * irho;
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
         } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) a[k] = __ldg(aux + (size_t)c * D::NA + k);
         }
         return;
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __
     const double irho = rcp64(u[0]);
 #pragma unroll
     for (int d = 0; d < DIM; d++) a[1 + d] = u[2 + d] * irho;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < NS; s++) a[1 + DIM + s] = u[D::NE + s] * irho;
     if (!ok) atomicOr(status, kStatusEos);
 }
@@ -324,7 +324,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
     using S = StateOf<G>;
     G phi[D::NC];
     int ist[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         phi[k] = big_value<G>();
         ist[k] = -1;
@@ -337,7 +337,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
         for (int d = 0; d < DIM; d++) v[d] = geo<G>(M.cv, M.cv32, 3 * (wb + (size_t)(i - beg)) + d);
         S un[D::NC];
         if (!sd) load_state<DIM, NS, S>(U, dU, M.cone[i].y & kConeNbr, un);
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             if (k < k0 || k >= k1) continue;
             G denom = 0;
@@ -358,12 +358,12 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
     }
     if constexpr (std::is_same<G, Dual>::value) {
         if (P.jvp_frozen_limiter) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) phi[k].d = 0.0;
         }
     }
     bool cancel = false;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         if (k < k0 || k >= k1) continue;
         if (phi[k] == G(0)) {
@@ -372,7 +372,7 @@ __device__ __forceinline__ void limit_field(const DevMesh& M, const Phys& P, int
                 if (dabs(g[k * DIM + d]) > G(P.max_lim_grad)) cancel = true;
         }
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) {
         if (k < k0 || k >= k1) continue;
         if constexpr (REC) {
@@ -410,9 +410,9 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
     load_state<DIM, NS, S>(U, dU, c, uc);
     if (auxg) cell_aux<DIM, NS>(P, uc, aux, c, ac);
     G g[D::NC * DIM], ga[D::NA * DIM];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC * DIM; k++) g[k] = G(0);
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NA * DIM; k++) ga[k] = G(0);
     // neighbour differences kept for the limiter when the block has shared memory for them
     G* sd = (cache && state && P.limiter != ABL_LIMITER_NONE && end - beg <= M.max_cone) ? reinterpret_cast<G*>(gsm) : nullptr;
@@ -424,13 +424,13 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
             S un[D::NC];
             if (state || !nasa || std::is_same<S, Dual>::value) load_state<DIM, NS, S>(U, dU, n, un);
             if (sd) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) sd[((i - beg) * D::NC + k) * blockDim.x + threadIdx.x] = G(un[k] - uc[k]);
             }
             G wd[DIM], wad[DIM];
             cone_weights<DIM, G>(M.cwa, M.cwa32, wb + (size_t)(i - beg), wd, wad);
             if (state && !(ce.y & kConeBoundary)) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) {
                     const G delta = G(un[k] - uc[k]);
 #pragma unroll
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
             if (auxg) {
                 S an[D::NA];
                 cell_aux<DIM, NS>(P, un, aux, n, an);
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NA; k++) {
                     const G delta = G(an[k] - ac[k]);
 #pragma unroll
@@ -452,14 +452,14 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
             // the unlimited gradient, and the limiter's factor and minimising face per component
             double ph[D::NC];
             int is[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) {
                 ph[k] = 1.0;
                 is[k] = -1;
             }
             if (do_state) {
                 G* o = graw + (size_t)c * GR::GS;
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC * DIM; k++) o[k] = g[k];
             }
             if (state && P.limiter != ABL_LIMITER_NONE) {
@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                 if (NS > 0) limit_field<DIM, NS, G, LIM, true>(M, P, beg, end, wb, U, dU, uc, g, D::NE, D::NC, ph, is, sd);
             }
             if (do_state) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) {
                     rphi[(size_t)c * D::NC + k] = ph[k];
                     rist[(size_t)c * D::NC + k] = is[k];
@@ -480,12 +480,12 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
     }
     if (do_state) {
         G* out = grad + (size_t)c * GR::GS;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC * DIM; k++) out[k] = g[k];
     }
     if (do_aux) {
         G* out = agrad + (size_t)c * GR::AS;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NA * DIM; k++) out[k] = ga[k];
     }
 }
@@ -554,7 +554,7 @@ __device__ __forceinline__ void advection_split(const Phys& P, const double* nor
     }
     if (spadv) {
         const double* u = us[s];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < NS; k++) flux[D::NE + k] = mA * (u[D::NE + k] * irho[s]);
     }
 }
@@ -580,7 +580,7 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
                                           bool* ok, bool* rok) {
     using D = Dims<DIM, NS>;
     using S = StateOf<G>;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) flux[k] = 0.0;
     S cL[D::NC], cR[D::NC];
     src.state(L, cL);
@@ -591,7 +591,7 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
         const bool lsq = P.recon == ABL_RECON_LEASTSQUARES;
         // ProjectToFace (cellInterpolant.cpp:890-950): cells with a gradient are projected to the face
         S uL[D::NC], uR[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             uL[k] = cL[k];
             uR[k] = cR[k];
@@ -601,7 +601,7 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
             G gL[D::NC * DIM], gR[D::NC * DIM];
             src.grad_row(L, gL);
             src.grad_row(R, gR);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) {
                 G dotL = 0, dotR = 0;
 #pragma unroll
@@ -688,14 +688,14 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
                 // SpeciesTransport::AdvectionFlux (speciesTransport.cpp:263-341): LEFT upwinds, anything else takes the right
                 // state; the compact process averages where there is no direction (compactCompressibleNSSpeciesTransport.cpp:257-259)
                 if (dir == ABL_DIR_LEFT) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int s = 0; s < NS; s++) flux[D::NE + s] = (mf * uL[D::NE + s] * irhoL) * areaMag;
                 } else if (dir == ABL_DIR_NA && P.sp_compact) {
                     const S rhoM = 0.5 * (uL[0] + uR[0]);
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int s = 0; s < NS; s++) flux[D::NE + s] = mf * 0.5 * (uR[D::NE + s] + uL[D::NE + s]) / rhoM * areaMag;
                 } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int s = 0; s < NS; s++) flux[D::NE + s] = (mf * uR[D::NE + s] * irhoR) * areaMag;
                 }
             }
@@ -709,9 +709,9 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
         S fs[D::NC], fa[D::NA], aL[D::NA], aR[D::NA];
         src.aux_of(P, cL, L, aL);
         src.aux_of(P, cR, R, aR);
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) fs[k] = cL[k] * 0.5 + cR[k] * 0.5;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NA; k++) fa[k] = aL[k] * 0.5 + aR[k] * 0.5;
         G gL[D::NA * DIM], gR[D::NA * DIM];
         if constexpr (DIM == 1) {
@@ -719,7 +719,7 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
             // the averages below return it exactly
             double wl, wr;
             face_weights_1d(fdx, &wl, &wr);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NA; k++) gL[k] = gR[k] = static_cast<G>(aL[k] * wl + aR[k] * wr);
         } else {
             src.agrad_row(L, gL);
@@ -768,15 +768,15 @@ __device__ __forceinline__ void face_flux(const Phys& P, const Src& src, int L, 
                 const S density = fs[0];
                 S hs[NS];
                 if (P.eos == ABL_EOS_NASA7) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int s = 0; s < NS; s++) hs[s] = nasa_h_molar(P.nasa7 + 15 * s, fa[0]) * P.inv_mw[s] - P.href[s];
                 } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
                     for (int s = 0; s < NS; s++) hs[s] = 0.0;
                 }
                 const int yoff = (1 + DIM) * DIM;
                 S ef = 0;
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int s = 0; s < NS; ++s) {
                     S sf = 0;
                     const S Ds = P.diff_k ? S(P.diff_k[s]) : diff;
@@ -855,7 +855,7 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
         S flux[D::NC];
         face_flux<DIM, NS, G, FK>(P, src, lr.x, lr.y, normal, fdx, flux, &ok, &rok);
         S* out = sflux + (size_t)(i - fb) * D::NC;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) out[k] = flux[k];
     }
     __syncthreads();
@@ -866,10 +866,10 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
         const double iv = M.ivol[c];
         S acc[D::NC];
         if (overwrite) {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) acc[k] = 0.0;
         } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) {
                 if constexpr (std::is_same<S, Dual>::value)
                     acc[k] = Dual(F ? F[(size_t)c * D::NC + k] : 0.0, dF[(size_t)c * D::NC + k]);
@@ -881,23 +881,23 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::tile) k_tile_flux(DevMe
         // exactly (a uniform state keeps a zero residual, as the reference's per-face division gives;
         // a per-face fma(flux, 1/V, acc) would leave the rounding error of the product instead)
         S sum[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) sum[k] = 0.0;
         const int e0 = M.tc_fptr[j], e1 = M.tc_fptr[j + 1];
         for (int e = e0; e < e1; e++) {
             const uint16_t code = M.tc_face[e];
             const S* ff = sflux + (size_t)(code & 0x7fff) * D::NC;
             if (code & 0x8000) {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) sum[k] += ff[k];
             } else {
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) sum[k] -= ff[k];
             }
         }
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) acc[k] += sum[k] * iv;
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             if constexpr (std::is_same<S, Dual>::value) {
                 if (F) F[(size_t)c * D::NC + k] = acc[k].v;

@@ -100,7 +100,16 @@ void launch_gradient(abl_fv* fv, const double* U, const double* dU, G* grad, G* 
 template <int DIM, int NS, class G>
 void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int overwrite, cudaStream_t s) {
     const Phys& P = fv->phys;
-    if (fv->fused_ok[std::is_same<G, float>::value ? 1 : 0]) {
+    if constexpr (!kSpecialized<NS>) {
+        // a capacity instance: generic limiter and flux calculator
+        if (fv->need_state_grad || fv->need_aux_grad) {
+            mark(fv, "k_gradient", s);
+            launch_gradient<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, s);
+        }
+        mark(fv, "k_tile_flux", s);
+        if (fv->mesh.n_tiles > 0) launch_tile<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
+        return;
+    } else if (fv->fused_ok[std::is_same<G, float>::value ? 1 : 0]) {
         mark(fv, "k_fused_rhs", s);
         if (fv->mesh.n_tiles > 0) {
             if (P.flux == ABL_FLUX_AUSMPUP) {
@@ -200,7 +209,9 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
     GradRec rec{fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p};
     if (fv->need_state_grad || fv->need_aux_grad) {
         mark(fv, "k_gradient", s);
-        auto kern = P.limiter == ABL_LIMITER_MINMOD ? k_gradient<DIM, NS, double, ABL_LIMITER_MINMOD, true> : k_gradient<DIM, NS, double, -1, true>;
+        auto kern = k_gradient<DIM, NS, double, -1, true>;
+        if constexpr (kSpecialized<NS>)
+            if (P.limiter == ABL_LIMITER_MINMOD) kern = k_gradient<DIM, NS, double, ABL_LIMITER_MINMOD, true>;
         const size_t smem = gradient_smem<DIM, NS, double>(fv);
         kern<<<blocks_for(M.n_cells, 128), 128, smem, s>>>(M, P, U, nullptr, fv->aux.p, fv->grad64.p, fv->agrad64.p, fv->need_state_grad,
                                                           fv->need_aux_grad, smem > 0, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p);
@@ -216,11 +227,13 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
         if (smem > 227 * 1024) throw AblError(ABL_ERR_UNSUPPORTED, "adjoint accumulators exceed shared memory for this species count");
         // flux calculator and limiter fixed at compile time where a specialised kernel exists
         auto kern = k_tile_adjoint<DIM, NS, -1, -1>;
-        if (P.flux == ABL_FLUX_AUSMPUP)
-            kern = P.limiter == ABL_LIMITER_MINMOD ? k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, ABL_LIMITER_MINMOD>
-                                                   : k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, -1>;
-        else if (P.flux == ABL_FLUX_AUSM)
-            kern = k_tile_adjoint<DIM, NS, ABL_FLUX_AUSM, -1>;
+        if constexpr (kSpecialized<NS>) {
+            if (P.flux == ABL_FLUX_AUSMPUP)
+                kern = P.limiter == ABL_LIMITER_MINMOD ? k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, ABL_LIMITER_MINMOD>
+                                                       : k_tile_adjoint<DIM, NS, ABL_FLUX_AUSMPUP, -1>;
+            else if (P.flux == ABL_FLUX_AUSM)
+                kern = k_tile_adjoint<DIM, NS, ABL_FLUX_AUSM, -1>;
+        }
         ABL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         static_assert(2 * kColorCap == 256, "one colour per pass of the 256-thread adjoint CTA");
         kern<<<M.n_tiles, 256, smem, s>>>(M, P, U, fv->aux.p, fv->grad64.p, fv->agrad64.p, Fb, rec, out, fv->adj_nb.p, ds, da, fv->status.p);

@@ -38,11 +38,11 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(GhostBC G, double* __restri
     const int g = G.cell[j], i = G.nbr[j];
     const abl_bc bc = G.table[G.bc[j]];
     double u[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) u[k] = U[(size_t)i * D::NC + k];
     switch (bc.kind) {
         case ABL_BC_DIRICHLET:
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) u[k] = bc.enforce_at_face ? (LIN ? 0.0 : 2.0 * bc.value[k]) - u[k] : (LIN ? 0.0 : bc.value[k]);
             break;
         case ABL_BC_SLIP_WALL: {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(GhostBC G, double* __restri
         default:  // ABL_BC_OUTFLOW: zero gradient
             break;
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) U[(size_t)g * D::NC + k] = u[k];
 }
 
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_normalize_species(DevMesh M, double* __
     const double density = u[0];
     double* rY = u + D::NE;
     double yiSum = 0.0;
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int s = 0; s < NS - 1; s++) {
         double yi = rY[s] / density;
         yi = pmax(0.0, yi);
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) k_normalize_species(DevMesh M, double* __
         rY[s] = yi * density;
     }
     if (yiSum > 1.0) {
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int s = 0; s < NS; s++) {
             double yi = rY[s] / density;
             yi /= yiSum;
@@ -177,24 +177,24 @@ __global__ void __launch_bounds__(256) k_fill_ghosts_vjp(GhostBC G, GhostSegment
     if (sidx >= S.n) return;
     const int i = S.nbr[sidx];
     double acc[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) acc[k] = 0.0;
     for (int q = S.ptr[sidx]; q < S.ptr[sidx + 1]; q++) {
         const int j = S.ghost[q];
         const int g = G.cell[j];
         const abl_bc bc = G.table[G.bc[j]];
         double lg[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) {
             lg[k] = Ub[(size_t)g * D::NC + k];
             Ub[(size_t)g * D::NC + k] = 0.0;
         }
         double vb[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) vb[k] = 0.0;
         switch (bc.kind) {
             case ABL_BC_DIRICHLET:
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) {
                     vb[k] = bc.enforce_at_face ? 2.0 * lg[k] : lg[k];
                     if (bc.enforce_at_face) acc[k] -= lg[k];
@@ -207,23 +207,23 @@ __global__ void __launch_bounds__(256) k_fill_ghosts_vjp(GhostBC G, GhostSegment
                 for (int d = 0; d < DIM; d++) mn += lg[2 + d] * G.normal[3 * (size_t)j + d];
 #pragma unroll
                 for (int d = 0; d < DIM; d++) lg[2 + d] -= 2.0 * mn * G.normal[3 * (size_t)j + d];
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) acc[k] += lg[k];
                 break;
             }
             case ABL_BC_NOSLIP_WALL:
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) acc[k] += (k >= 2 && k < 2 + DIM) ? -lg[k] : lg[k];
                 break;
             default:
-#pragma unroll
+ABL_UNROLL_SPECIES
                 for (int k = 0; k < D::NC; k++) acc[k] += lg[k];
                 break;
         }
-#pragma unroll
+ABL_UNROLL_SPECIES
         for (int k = 0; k < D::NC; k++) vbar[(size_t)j * D::NC + k] = vb[k];
     }
-#pragma unroll
+ABL_UNROLL_SPECIES
     for (int k = 0; k < D::NC; k++) Ub[(size_t)i * D::NC + k] += acc[k];
 }
 
@@ -269,10 +269,10 @@ __global__ void __launch_bounds__(256) k_pressure_functional(Phys P, int n, cons
         if (!ok) atomicOr(status, kStatusEos);
         if (Ub) {
             double ub[D::NC];
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) ub[k] = 0.0;
             decode_vjp<DIM, NS>(P, NS, u, dd, 0.0, 0.0, w[j], ub);
-#pragma unroll
+ABL_UNROLL_SPECIES
             for (int k = 0; k < D::NC; k++) Ub[(size_t)c * D::NC + k] += ub[k];
         }
     }

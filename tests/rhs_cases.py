@@ -84,6 +84,17 @@ def case(name: str) -> Workload:
             tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
         procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
         return Workload(name, mesh, eos, procs, "leastsquares", "vanleer", U, name)
+    if name == "gri30_box3d":
+        # the reference's 53-species gri30 thermodynamics (the input of its tChemTests.cpp) on a small
+        # box: a count without an instance of its own, run padded in the largest species instance
+        from tests import golden_cases as G
+        mesh = box_mesh((5, 4, 3), lower=(0, 0, 0), upper=(0.5, 0.4, 0.3), periodic=(True, False, False))
+        eos = G.gri30_eos()
+        U = _perturbed_state(mesh, rng, 3, len(eos.GetSpeciesVariables()), eos)
+        flux = fv.AusmpUp(0.3)
+        tr = fv.ConstantLewis(1.8e-5, 0.72, 1.0)
+        procs = [fv.NavierStokesTransport({}, eos, flux, tr), fv.SpeciesTransport(eos, flux, tr)]
+        return Workload(name, mesh, eos, procs, "leastsquares", "minmod", U, name)
     if name == "compact3d_avg_ns5":
         # the compact NS + species process with the average flux (no direction: the averaged species
         # advection), per-species diffusivities
