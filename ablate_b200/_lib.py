@@ -39,6 +39,7 @@ BC_MAX_COMPONENTS = 16
 JVP_EXACT, JVP_FROZEN_LIMITER = 0, 1
 STEP_EULER, STEP_SSPRK3 = 0, 1
 RHS_OVERWRITE = 0x100
+RHS_PHASE_INTERIOR, RHS_PHASE_REST = 0, 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -81,6 +82,7 @@ SIGNATURES = {
     "abl_fv_fused_info": (C.c_int, [C.c_void_p, _ip, _ip, _ip, _ip]),
     "abl_fv_rhs": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "abl_fv_rhs_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, C.c_int]),
+    "abl_fv_rhs_phase": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "abl_fv_jvp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "abl_fv_jvp_host": (C.c_int, [C.c_void_p, C.c_double, _dp, _dp, _dp, _dp]),
     "abl_fv_vjp": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

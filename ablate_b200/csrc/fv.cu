@@ -659,6 +659,22 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             fv->wsum.upload(ws.data(), ws.size());
         }
 
+        {
+            // the two parts of a split RHS: the cells that need no halo row (their aux, and the gradients
+            // whose stencils hold none) and the rest
+            std::vector<int32_t> ae, al, ge, gl;
+            for (int c = 0; c < h.n_cells; c++) {
+                const auto is_halo = [&](int x) { return h.kind[x] == ABL_CELL_HALO || h.kind[x] == ABL_CELL_HALO_OUTER; };
+                bool early = !is_halo(c);
+                (early ? ae : al).push_back(c);
+                for (int i = h.cone_ptr[c]; i < h.cone_ptr[c + 1] && early; i++) early = !is_halo(h.cone_nbr[i]);
+                (early ? ge : gl).push_back(c);
+            }
+            fv->aux_early.upload(ae.data(), ae.size());
+            fv->aux_late.upload(al.data(), al.size());
+            fv->grad_early.upload(ge.data(), ge.size());
+            fv->grad_late.upload(gl.data(), gl.size());
+        }
         fv->aux.alloc((size_t)fv->n_cells * fv->naux);
         {
             std::vector<double> a0((size_t)fv->n_cells * fv->naux, 0.0);
@@ -851,6 +867,28 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
         double* F = pad_out(fv, fv->pF, s);
         dispatch_rhs(fv, U, F, precision, 1, s);
         unpad_rows(fv, F, F_dev, true, !overwrite, s);
+    });
+}
+
+int abl_fv_rhs_phase(abl_fv* fv, double time, const double* U_dev, double* F_dev, int precision, int phase, void* stream) {
+    struct PhaseOff {
+        abl_fv* fv;
+        ~PhaseOff() { fv->rhs_phase = -1; }
+    };
+    return guarded([&] {
+        if (!fv || !U_dev || !F_dev) throw std::invalid_argument("abl_fv_rhs_phase: NULL argument");
+        if (phase != ABL_RHS_PHASE_INTERIOR && phase != ABL_RHS_PHASE_REST) throw std::invalid_argument("abl_fv_rhs_phase: unknown phase");
+        if (fv->pad) {
+            // a padded count converts every row at once: everything runs in the second phase
+            if (phase == ABL_RHS_PHASE_INTERIOR) return;
+            const int rc = abl_fv_rhs(fv, time, U_dev, F_dev, precision, stream);
+            if (rc != ABL_OK) throw AblError(rc, g_last_error);
+            return;
+        }
+        PhaseOff off{fv};
+        fv->rhs_phase = phase;
+        const int rc = abl_fv_rhs(fv, time, U_dev, F_dev, precision, stream);
+        if (rc != ABL_OK) throw AblError(rc, g_last_error);
     });
 }
 

@@ -155,6 +155,10 @@ struct abl_fv {
     bool pipe_active = false;          // set for the duration of one abl_fv_rhs_host call
     double* pipe_F_host = nullptr;
     bool need_aux = false, need_state_grad = false, need_aux_grad = false;
+    // split RHS (abl_fv_rhs_phase): -1 the whole RHS; 0 the aux update and gradients of the cells whose
+    // stencils hold no halo row; 1 the rest. Cell lists of the two parts:
+    int rhs_phase = -1;
+    abl::DevBuf<int> aux_early, aux_late, grad_early, grad_late;
 };
 
 namespace abl {

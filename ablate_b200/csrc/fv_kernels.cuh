@@ -291,11 +291,14 @@ struct GlobalRows {
 };
 
 // ---------------------------------------------------------------------------------------------------
+// cells: the listed cells only (n_list of them), or every cell when null
 template <int DIM, int NS>
-__global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __restrict__ U, double* __restrict__ aux, int* status) {
+__global__ void __launch_bounds__(256) k_aux(DevMesh M, Phys P, const double* __restrict__ U, double* __restrict__ aux, int* status,
+                                             const int* __restrict__ cells = nullptr, int n_list = 0) {
     using D = Dims<DIM, NS>;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= M.n_cells) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (cells ? n_list : M.n_cells)) return;
+    const int c = cells ? __ldg(cells + i) : i;
     double u[D::NC];
     load_state<DIM, NS>(U, c, u);
     double* a = aux + (size_t)c * D::NA;
@@ -393,13 +396,16 @@ __global__ void __launch_bounds__(128, MinBlocks<NS, G>::grad) k_gradient(DevMes
                                                                     const double* __restrict__ dU, const double* __restrict__ aux,
                                                                     G* __restrict__ grad, G* __restrict__ agrad, int do_state, int do_aux,
                                                                     int cache, G* __restrict__ graw = nullptr, double* __restrict__ rphi = nullptr,
-                                                                    int* __restrict__ rist = nullptr) {
+                                                                    int* __restrict__ rist = nullptr, const int* __restrict__ cells = nullptr,
+                                                                    int n_list = 0) {
     extern __shared__ __align__(16) unsigned char gsm[];
     using D = Dims<DIM, NS>;
     using GR = GradRows<DIM, NS, G>;
     using S = StateOf<G>;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= M.n_cells) return;
+    // cells: the listed cells only (n_list of them), or every cell when null
+    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= (cells ? n_list : M.n_cells)) return;
+    const int c = cells ? __ldg(cells + ci) : ci;
     const uint8_t kind = M.kind[c];
     const int beg = M.cone_ptr[c], end = M.cone_ptr[c + 1];
     const size_t wb = weight_base(M, c, beg);

@@ -87,11 +87,25 @@ size_t gradient_smem(const abl_fv* fv) {
     return b <= 48 * 1024 ? b : 0;
 }
 
+// the gradient pass over every cell, or (split RHS) over the phase's cells
 template <int DIM, int NS, class G, int LIM>
 void launch_gradient(abl_fv* fv, const double* U, const double* dU, G* grad, G* agrad, cudaStream_t s) {
     const size_t smem = gradient_smem<DIM, NS, G>(fv);
-    k_gradient<DIM, NS, G, LIM><<<blocks_for(fv->mesh.n_cells, 128), 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad,
-                                                                                  fv->need_state_grad, fv->need_aux_grad, smem > 0);
+    const abl::DevBuf<int>* list = fv->rhs_phase == 0 ? &fv->grad_early : fv->rhs_phase == 1 ? &fv->grad_late : nullptr;
+    const int n = list ? (int)list->n : fv->mesh.n_cells;
+    if (n == 0) return;
+    k_gradient<DIM, NS, G, LIM><<<blocks_for(n, 128), 128, smem, s>>>(fv->mesh, fv->phys, U, dU, fv->aux.p, grad, agrad, fv->need_state_grad,
+                                                                   fv->need_aux_grad, smem > 0, nullptr, nullptr, nullptr, list ? list->p : nullptr, n);
+    check_launch();
+}
+
+// the aux update over every cell, or (split RHS) over the phase's cells
+template <int DIM, int NS>
+void launch_aux(abl_fv* fv, const double* U, cudaStream_t s) {
+    const abl::DevBuf<int>* list = fv->rhs_phase == 0 ? &fv->aux_early : fv->rhs_phase == 1 ? &fv->aux_late : nullptr;
+    const int n = list ? (int)list->n : fv->mesh.n_cells;
+    if (n == 0) return;
+    k_aux<DIM, NS><<<blocks_for(n, 256), 256, 0, s>>>(fv->mesh, fv->phys, U, fv->aux.p, fv->status.p, list ? list->p : nullptr, n);
     check_launch();
 }
 
@@ -107,9 +121,11 @@ void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int ove
             launch_gradient<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, s);
         }
         mark(fv, "k_tile_flux", s);
-        if (fv->mesh.n_tiles > 0) launch_tile<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
+        if (fv->mesh.n_tiles > 0 && fv->rhs_phase != 0) launch_tile<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
         return;
     } else if (fv->fused_ok[std::is_same<G, float>::value ? 1 : 0]) {
+        // one pass over everything: nothing in the first phase of a split RHS
+        if (fv->rhs_phase == 0) return;
         mark(fv, "k_fused_rhs", s);
         if (fv->mesh.n_tiles > 0) {
             if (P.flux == ABL_FLUX_AUSMPUP) {
@@ -133,7 +149,7 @@ void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int ove
             launch_gradient<DIM, NS, G, -1>(fv, U, nullptr, grad, agrad, s);
     }
     mark(fv, "k_tile_flux", s);
-    if (fv->mesh.n_tiles > 0) {
+    if (fv->mesh.n_tiles > 0 && fv->rhs_phase != 0) {
         if (P.flux == ABL_FLUX_AUSMPUP)
             launch_tile<DIM, NS, G, ABL_FLUX_AUSMPUP>(fv, U, nullptr, grad, agrad, F, nullptr, overwrite, s);
         else if (P.flux == ABL_FLUX_AUSM)
@@ -145,12 +161,10 @@ void rhs_with(abl_fv* fv, const double* U, G* grad, G* agrad, double* F, int ove
 
 template <int DIM, int NS>
 void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
-    const DevMesh& M = fv->mesh;
     fv->n_marks = 0;
     if (fv->need_aux) {
         mark(fv, "k_aux", s);
-        k_aux<DIM, NS><<<blocks_for(M.n_cells, 256), 256, 0, s>>>(M, fv->phys, U, fv->aux.p, fv->status.p);
-        check_launch();
+        launch_aux<DIM, NS>(fv, U, s);
     }
     // With species the mixed request runs the FP64 kernels: the NASA-7 decode (FP64 by design) dominates
     // their cost, and FP32 gradients of steep temperature / composition layers exceed the 1e-6 error
@@ -214,7 +228,7 @@ void run_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStre
             if (P.limiter == ABL_LIMITER_MINMOD) kern = k_gradient<DIM, NS, double, ABL_LIMITER_MINMOD, true>;
         const size_t smem = gradient_smem<DIM, NS, double>(fv);
         kern<<<blocks_for(M.n_cells, 128), 128, smem, s>>>(M, P, U, nullptr, fv->aux.p, fv->grad64.p, fv->agrad64.p, fv->need_state_grad,
-                                                          fv->need_aux_grad, smem > 0, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p);
+                                                          fv->need_aux_grad, smem > 0, fv->adj_graw.p, fv->adj_phi.p, fv->adj_ist.p, nullptr, 0);
         check_launch();
     }
     AdjOut<DIM, NS> out{fv->need_state_grad ? fv->adj_gb.p : nullptr, fv->adj_beta.p, fv->adj_fstar.p,

@@ -274,12 +274,29 @@ class DistributedRHS:
         distributed = dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1
         plan = plan_with(dom, group) if distributed else ExchangePlan({}, {})
         self.halo = HaloExchange(plan, self.solver.nc, self.device, group)
+        self.comm_stream = None  # created on the first overlapped exchange
 
-    def ComputeRHSDevice(self, time: float, U, F, precision: int = L.PRECISION_FP64):
-        """F += RHS(U) on the owned rows after refreshing U's halo rows; U, F torch tensors on this GPU."""
-        self.halo.exchange(U)
-        stream = self.torch.cuda.current_stream(self.device).cuda_stream
-        self.solver.ComputeRHSDevice(time, U.data_ptr(), F.data_ptr(), precision, stream)
+    def ComputeRHSDevice(self, time: float, U, F, precision: int = L.PRECISION_FP64, overlap: bool = True):
+        """F += RHS(U) on the owned rows after refreshing U's halo rows; U, F torch tensors on this GPU.
+
+        With overlap, the exchange runs on a second stream while the current one computes the part of the
+        RHS that reads no halo row (abl_fv_rhs_phase, interior phase); the rest follows once the exchange
+        is done. The exchange writes only halo rows and the interior phase reads none, so the two overlap
+        without a race, and the residual equals the serial order's bit for bit."""
+        torch = self.torch
+        cur = torch.cuda.current_stream(self.device)
+        if not overlap or not self.halo.peers:
+            self.halo.exchange(U)
+            self.solver.ComputeRHSDevice(time, U.data_ptr(), F.data_ptr(), precision, cur.cuda_stream)
+            return
+        if self.comm_stream is None:
+            self.comm_stream = torch.cuda.Stream(self.device)
+        self.comm_stream.wait_stream(cur)  # U is written before the exchange packs it
+        with torch.cuda.stream(self.comm_stream):
+            self.halo.exchange(U)
+        self.solver.ComputeRHSPhaseDevice(time, U.data_ptr(), F.data_ptr(), L.RHS_PHASE_INTERIOR, precision, cur.cuda_stream)
+        cur.wait_stream(self.comm_stream)
+        self.solver.ComputeRHSPhaseDevice(time, U.data_ptr(), F.data_ptr(), L.RHS_PHASE_REST, precision, cur.cuda_stream)
 
     def ComputeJVPDevice(self, time: float, U, dU, dF, F=None):
         """dF += J(U) dU on the owned rows (and F += RHS(U) when F is given), after refreshing the halo

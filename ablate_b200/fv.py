@@ -372,6 +372,12 @@ class FiniteVolumeSolver:
         """F += RHS(U) with device pointers (e.g. torch tensors' data_ptr()), enqueued on `stream`."""
         L.check(L.lib.abl_fv_rhs(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(F_ptr), precision, C.c_void_p(stream)), "abl_fv_rhs")
 
+    def ComputeRHSPhaseDevice(self, time: float, U_ptr: int, F_ptr: int, phase: int, precision: int = L.PRECISION_FP64, stream: int = 0):
+        """One phase of a split RHS (L.RHS_PHASE_INTERIOR reads no halo row; L.RHS_PHASE_REST, after the
+        halo rows are current, finishes it): the two in order equal ComputeRHSDevice."""
+        L.check(L.lib.abl_fv_rhs_phase(self.handle, time, C.c_void_p(U_ptr), C.c_void_p(F_ptr), precision, phase, C.c_void_p(stream)),
+                "abl_fv_rhs_phase")
+
     def ComputeJVP(self, time: float, locX: np.ndarray, dX: np.ndarray, dF: np.ndarray, F: np.ndarray | None = None):
         """dF += J(locX) dX (and F += RHS(locX) when F is given), host arrays (n_cells, nc)."""
         x = np.ascontiguousarray(locX, dtype=np.float64)

@@ -133,9 +133,13 @@ typedef struct abl_physics_desc {
     int32_t eos;             /* ABL_EOS_* */
     double gamma;            /* perfect gas: specific heat ratio (default 1.4) */
     double r_gas;            /* perfect gas: gas constant J/(kg K) (default 287) */
-    int32_t n_species;       /* densityYi components; 0 = no species field. Compiled (dim, n_species):
-                                (1, 0), (2, 0), (2, 2), (2, 3), (3, 0), (3, 2), (3, 5), (3, 9); others give
-                                ABL_ERR_UNSUPPORTED at create */
+    int32_t n_species;       /* densityYi components, 0..128; 0 = no species field. Instances with their
+                                loops unrolled: (1, 0), (2, 0), (2, 2), (2, 3), (3, 0), (3, 2), (3, 5),
+                                (3, 9); with run-time loops: 16 and 128 species in 1D, 2D and 3D. Any other
+                                count runs in the smallest instance that holds it, its species after zero-state
+                                padding species (results unchanged; the RHS, JVP, VJP and aux entry points
+                                translate the rows; the ghost, step and functional entry points return
+                                ABL_ERR_UNSUPPORTED for such a count) */
     const double* nasa7;     /* [n_species][15]: T_mid, low a1..a7, high a1..a7 (cp/R = a1 + a2 T + ... ) */
     const double* mw;        /* [n_species] molar mass kg/kmol */
 
@@ -210,6 +214,18 @@ int abl_fv_rhs(abl_fv* fv, double time, const double* U_dev, double* F_dev, int 
  * rows of F travel when they are one contiguous range. Pinned host memory makes the copies asynchronous.
  * A handle serves one call at a time (no two threads on one handle). */
 int abl_fv_rhs_host(abl_fv* fv, double time, const double* U_host, double* F_host, int precision);
+
+/* abl_fv_rhs in two phases, so that a partitioned run moves its halo while the device computes. Phase
+ * ABL_RHS_PHASE_INTERIOR reads no halo row (ABL_CELL_HALO, ABL_CELL_HALO_OUTER): it updates the aux
+ * fields of the other cells and the gradients of the cells whose stencils hold no halo cell. Phase
+ * ABL_RHS_PHASE_REST, issued after the halo rows are current, does the rest and adds the residual into
+ * F. The two calls on one stream equal one abl_fv_rhs call bit for bit; the caller may write the halo
+ * rows of U between them (the exchange of DMGlobalToLocal, src/solver/timeStepper.cpp:343-344, moved
+ * beside the interior work). Kernels that do not split (the fused kernel, a padded species count) run
+ * entirely in the second phase. */
+#define ABL_RHS_PHASE_INTERIOR 0
+#define ABL_RHS_PHASE_REST 1
+int abl_fv_rhs_phase(abl_fv* fv, double time, const double* U_dev, double* F_dev, int precision, int phase, void* stream);
 
 /* Forward tangent (JVP) of abl_fv_rhs at FP64: dF += J(U) dU for owned cells, and F += RHS(U) when F
  * is not NULL. The RHS kernels are evaluated on dual numbers (value + one directional derivative), so
