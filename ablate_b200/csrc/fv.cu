@@ -140,41 +140,73 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
 }
 
 // ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
-// Exact species counts (fv_inst_*.cu, fv_adj_*.cu) and the capacity instances 16 and kMaxSpecies
-// (fv_inst_cap.cu, fv_adj_cap.cu), per dimension, ascending.
+// Exact species counts (fv_inst_a..d.cu, fv_adj_*.cu), the 16-species instances (fv_inst_e.cu,
+// fv_inst_f.cu: RHS, aux update, tangent) and the kMaxSpecies capacity instances (fv_inst_cap.cu: RHS
+// and aux update, run-time loops), per dimension, ascending.
 constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSpecies, -1}, {0, 2, 3, 5, 9, 16, kMaxSpecies, -1}};
 
-#define ABL_DISPATCH(fv, FN, ...)                                                                                                  \
-    do {                                                                                                                           \
-        switch ((fv)->dim * 1000 + (fv)->ns) {                                                                                     \
-            case 1000: FN<1, 0>(fv, __VA_ARGS__); break;                                                                           \
-            case 1016: FN<1, 16>(fv, __VA_ARGS__); break;                                                                          \
-            case 1000 + kMaxSpecies: FN<1, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
-            case 2000: FN<2, 0>(fv, __VA_ARGS__); break;                                                                           \
-            case 2002: FN<2, 2>(fv, __VA_ARGS__); break;                                                                           \
-            case 2003: FN<2, 3>(fv, __VA_ARGS__); break;                                                                           \
-            case 2016: FN<2, 16>(fv, __VA_ARGS__); break;                                                                          \
-            case 2000 + kMaxSpecies: FN<2, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
-            case 3000: FN<3, 0>(fv, __VA_ARGS__); break;                                                                           \
-            case 3002: FN<3, 2>(fv, __VA_ARGS__); break;                                                                           \
-            case 3005: FN<3, 5>(fv, __VA_ARGS__); break;                                                                           \
-            case 3009: FN<3, 9>(fv, __VA_ARGS__); break;                                                                           \
-            case 3016: FN<3, 16>(fv, __VA_ARGS__); break;                                                                          \
-            case 3000 + kMaxSpecies: FN<3, kMaxSpecies>(fv, __VA_ARGS__); break;                                                   \
-            default: throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for this dimension/species count");          \
-        }                                                                                                                          \
+#define ABL_CASES_EXACT(FN, ...)                              \
+    case 1000: FN<1, 0>(fv, __VA_ARGS__); break;              \
+    case 2000: FN<2, 0>(fv, __VA_ARGS__); break;              \
+    case 2002: FN<2, 2>(fv, __VA_ARGS__); break;              \
+    case 2003: FN<2, 3>(fv, __VA_ARGS__); break;              \
+    case 3000: FN<3, 0>(fv, __VA_ARGS__); break;              \
+    case 3002: FN<3, 2>(fv, __VA_ARGS__); break;              \
+    case 3005: FN<3, 5>(fv, __VA_ARGS__); break;              \
+    case 3009: FN<3, 9>(fv, __VA_ARGS__); break;
+#define ABL_CASES_16(FN, ...)                                 \
+    case 1016: FN<1, 16>(fv, __VA_ARGS__); break;             \
+    case 2016: FN<2, 16>(fv, __VA_ARGS__); break;             \
+    case 3016: FN<3, 16>(fv, __VA_ARGS__); break;
+#define ABL_CASES_CAP(FN, ...)                                \
+    case 1000 + kMaxSpecies: FN<1, kMaxSpecies>(fv, __VA_ARGS__); break; \
+    case 2000 + kMaxSpecies: FN<2, kMaxSpecies>(fv, __VA_ARGS__); break; \
+    case 3000 + kMaxSpecies: FN<3, kMaxSpecies>(fv, __VA_ARGS__); break;
+
+// RHS and aux update: every instance
+#define ABL_DISPATCH(fv, FN, ...)                                                                                         \
+    do {                                                                                                                  \
+        switch ((fv)->dim * 1000 + (fv)->ns) {                                                                            \
+            ABL_CASES_EXACT(FN, __VA_ARGS__)                                                                              \
+            ABL_CASES_16(FN, __VA_ARGS__)                                                                                 \
+            ABL_CASES_CAP(FN, __VA_ARGS__)                                                                                \
+            default: throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for this dimension/species count"); \
+        }                                                                                                                 \
+    } while (0)
+// ghost fill, CFL, normalisation, stepping and the pressure functional: the exact counts (the callers
+// check require_exact_instance first)
+#define ABL_DISPATCH_EXACT(fv, FN, ...)                                                                                                \
+    do {                                                                                                                               \
+        switch ((fv)->dim * 1000 + (fv)->ns) {                                                                                         \
+            ABL_CASES_EXACT(FN, __VA_ARGS__)                                                                                           \
+            default: throw AblError(ABL_ERR_UNSUPPORTED, "this entry point has no compiled instance for this dimension/species count"); \
+        }                                                                                                                              \
     } while (0)
 
 void dispatch_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrite, cudaStream_t s) {
     ABL_DISPATCH(fv, run_rhs, U, F, precision, overwrite, s);
 }
 
+// the tangent: the exact counts and the 16-species instances (the capacity instance's run-time loops
+// are not compiled for dual numbers)
 void dispatch_jvp(abl_fv* fv, const double* U, const double* dU, double* F, double* dF, cudaStream_t s) {
-    ABL_DISPATCH(fv, run_jvp, U, dU, F, dF, s);
+    switch (fv->dim * 1000 + fv->ns) {
+        ABL_CASES_EXACT(run_jvp, U, dU, F, dF, s)
+        ABL_CASES_16(run_jvp, U, dU, F, dF, s)
+        default:
+            throw AblError(ABL_ERR_UNSUPPORTED, "the JVP is compiled for up to 16 species; " + std::to_string(fv->ns_user) + " species run in the " +
+                                                    std::to_string(fv->ns) + "-species instance, which has the RHS only");
+    }
 }
 
+// the adjoint: the exact counts (up to 9 species)
 void dispatch_vjp(abl_fv* fv, const double* U, const double* Fb, double* Ub, cudaStream_t s) {
-    ABL_DISPATCH(fv, run_vjp, U, Fb, Ub, s);
+    switch (fv->dim * 1000 + fv->ns) {
+        ABL_CASES_EXACT(run_vjp, U, Fb, Ub, s)
+        default:
+            throw AblError(ABL_ERR_UNSUPPORTED, "the VJP is compiled for the exact species counts (0, 2, 3 in 2D; 0, 2, 5, 9 in 3D); " +
+                                                    std::to_string(fv->ns_user) + " species run in the " + std::to_string(fv->ns) + "-species instance");
+    }
 }
 
 // The instance that runs ns species in dim dimensions: the smallest compiled one that holds them (-1:
@@ -242,11 +274,12 @@ void unpad_rows(abl_fv* fv, const double* inst, double* user, bool owned_only, b
                                                                            fv->pad, user, add ? 1 : 0);
     check_launch();
 }
-// entry points that work on the instance's rows directly need a count with an instance of its own
+// ghost fill, CFL, normalisation, stepping and the pressure functional are compiled for the exact
+// species counts only (0, 2, 3 in 2D; 0, 2, 5, 9 in 3D)
 void require_exact_instance(const abl_fv* fv, const char* what) {
-    if (fv->pad)
-        throw AblError(ABL_ERR_UNSUPPORTED, std::string(what) + ": " + std::to_string(fv->ns_user) +
-                                                " species run padded in a larger instance; this entry point needs a count with an instance of its own");
+    if (fv->pad || fv->ns > 9)
+        throw AblError(ABL_ERR_UNSUPPORTED, std::string(what) + ": " + std::to_string(fv->ns_user) + " species run in the " + std::to_string(fv->ns) +
+                                                "-species instance; this entry point is compiled for the exact counts (0, 2, 3 in 2D; 0, 2, 5, 9 in 3D)");
 }
 
 // ---- batch kernels ------------------------------------------------------------------------------
@@ -1354,7 +1387,7 @@ int abl_fv_fill_ghosts(abl_fv* fv, double time, double* U_dev, void* stream) {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_fill_ghosts: NULL argument");
         require_exact_instance(fv, "abl_fv_fill_ghosts");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, static_cast<cudaStream_t>(stream));
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U_dev, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -1371,7 +1404,7 @@ int abl_fv_fill_ghosts_jvp(abl_fv* fv, double* dU_dev, void* stream) {
         if (!fv || !dU_dev) throw std::invalid_argument("abl_fv_fill_ghosts_jvp: NULL argument");
         require_exact_instance(fv, "abl_fv_fill_ghosts_jvp");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_DISPATCH(fv, run_fill_ghosts_jvp, dU_dev, static_cast<cudaStream_t>(stream));
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts_jvp, dU_dev, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -1384,7 +1417,7 @@ int abl_fv_fill_ghosts_vjp(abl_fv* fv, double* Ubar_dev, double* value_bar_host,
         const size_t nv = (size_t)fv->n_bc * ABL_BC_MAX_COMPONENTS;
         if (fv->bc_vbar.n != nv) fv->bc_vbar.alloc(nv);
         ABL_CUDA(cudaMemsetAsync(fv->bc_vbar.p, 0, nv * sizeof(double), s));
-        ABL_DISPATCH(fv, run_fill_ghosts_vjp, Ubar_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts_vjp, Ubar_dev, s);
         if (value_bar_host) {
             std::vector<double> vb(nv);
             ABL_CUDA(cudaMemcpyAsync(vb.data(), fv->bc_vbar.p, nv * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1421,7 +1454,7 @@ int abl_fv_pressure_functional(abl_fv* fv, const double* U_dev, double* J_host, 
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         *J_host = 0.0;
         if (fv->fn_n == 0) return;
-        ABL_DISPATCH(fv, run_pressure_functional, U_dev, Ubar_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_pressure_functional, U_dev, Ubar_dev, s);
         std::vector<double> part(blocks_for(fv->fn_n, 256));
         ABL_CUDA(cudaMemcpyAsync(part.data(), fv->fn_partial.p, part.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         ABL_CUDA(cudaStreamSynchronize(s));
@@ -1438,7 +1471,7 @@ int abl_fv_cfl_dt(abl_fv* fv, const double* U_dev, double cfl, double* dt_host, 
         if (!(cfl > 0)) throw std::invalid_argument("abl_fv_cfl_dt: cfl must be positive");
         ABL_CUDA(cudaSetDevice(fv->device));
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        ABL_DISPATCH(fv, run_cfl_dt, U_dev, cfl, s);
+        ABL_DISPATCH_EXACT(fv, run_cfl_dt, U_dev, cfl, s);
         double dt = 0;
         ABL_CUDA(cudaMemcpyAsync(&dt, fv->dt_bits.p, sizeof(double), cudaMemcpyDeviceToHost, s));
         ABL_CUDA(cudaStreamSynchronize(s));
@@ -1451,7 +1484,7 @@ int abl_fv_normalize_species(abl_fv* fv, double* U_dev, void* stream) {
         if (!fv || !U_dev) throw std::invalid_argument("abl_fv_normalize_species: NULL argument");
         require_exact_instance(fv, "abl_fv_normalize_species");
         ABL_CUDA(cudaSetDevice(fv->device));
-        ABL_DISPATCH(fv, run_normalize, U_dev, static_cast<cudaStream_t>(stream));
+        ABL_DISPATCH_EXACT(fv, run_normalize, U_dev, static_cast<cudaStream_t>(stream));
     });
 }
 
@@ -1477,7 +1510,7 @@ int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, i
         if (fv->step_F.n != n) fv->step_F.alloc(n);
         double* F = fv->step_F.p;
         (void)time;
-        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U_dev, s);
         dispatch_rhs(fv, U_dev, F, precision, 1, s);
         if (scheme == ABL_STEP_EULER) {
             rk_stage(fv, 0.0, nullptr, 1.0, U_dev, dt, F, U_dev, s);
@@ -1487,15 +1520,15 @@ int abl_fv_step(abl_fv* fv, int scheme, double time, double dt, double* U_dev, i
             double* U1 = fv->step_U1.p;
             ABL_CUDA(cudaMemcpyAsync(U1, U_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
             rk_stage(fv, 0.0, nullptr, 1.0, U_dev, dt, F, U1, s);
-            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U1, s);
             dispatch_rhs(fv, U1, F, precision, 1, s);
             rk_stage(fv, 0.75, U_dev, 0.25, U1, dt, F, U1, s);
-            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U1, s);
             dispatch_rhs(fv, U1, F, precision, 1, s);
             rk_stage(fv, 1.0 / 3.0, U_dev, 2.0 / 3.0, U1, dt, F, U_dev, s);
         }
-        ABL_DISPATCH(fv, run_normalize, U_dev, s);
-        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_normalize, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U_dev, s);
     });
 }
 
@@ -1544,8 +1577,8 @@ int abl_fv_step_cfl(abl_fv* fv, int scheme, double cfl, double* U_dev, int preci
         if (fv->step_F.n != n) fv->step_F.alloc(n);
         double* F = fv->step_F.p;
         // the CFL step of the state the step starts from, as abl_fv_cfl_dt computes it (ghosts filled first)
-        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
-        ABL_DISPATCH(fv, run_cfl_dt, U_dev, cfl, s);
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_cfl_dt, U_dev, cfl, s);
         dispatch_rhs(fv, U_dev, F, precision, 1, s);
         if (scheme == ABL_STEP_EULER) {
             rk_stage_dev(fv, 0.0, nullptr, 1.0, U_dev, F, U_dev, time_dev, s);
@@ -1554,15 +1587,15 @@ int abl_fv_step_cfl(abl_fv* fv, int scheme, double cfl, double* U_dev, int preci
             double* U1 = fv->step_U1.p;
             ABL_CUDA(cudaMemcpyAsync(U1, U_dev, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
             rk_stage_dev(fv, 0.0, nullptr, 1.0, U_dev, F, U1, nullptr, s);
-            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U1, s);
             dispatch_rhs(fv, U1, F, precision, 1, s);
             rk_stage_dev(fv, 0.75, U_dev, 0.25, U1, F, U1, nullptr, s);
-            ABL_DISPATCH(fv, run_fill_ghosts, U1, s);
+            ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U1, s);
             dispatch_rhs(fv, U1, F, precision, 1, s);
             rk_stage_dev(fv, 1.0 / 3.0, U_dev, 2.0 / 3.0, U1, F, U_dev, time_dev, s);
         }
-        ABL_DISPATCH(fv, run_normalize, U_dev, s);
-        ABL_DISPATCH(fv, run_fill_ghosts, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_normalize, U_dev, s);
+        ABL_DISPATCH_EXACT(fv, run_fill_ghosts, U_dev, s);
     });
 }
 

@@ -22,7 +22,8 @@ constexpr int kColorCap = 128;
 constexpr int kMaxSpecies = 128;
 
 // Instances compiled with their flux calculator and limiter fixed at compile time (and the fused
-// kernel): the exact species counts up to 9. The capacity instances (16 and kMaxSpecies species, run-
+// kernel, the adjoint and the stepping kernels): the exact species counts up to 9. The 16-species
+// instances (RHS, aux update, tangent) and the kMaxSpecies capacity instances (RHS and aux update, run-
 // time loops) run the generic kernels only.
 template <int NS>
 constexpr bool kSpecialized = NS <= 9;
