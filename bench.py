@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-species-case", action="store_true",
-                    help="skip the 256^3 five-species case measured beside the Taylor-Green headline")
+                    help="skip the species cases (256^3 five species, 2M tetrahedra nine species) measured beside the Taylor-Green headline")
     return ap.parse_args()
 
 
@@ -298,18 +298,20 @@ def wall_studies(w, solver, U, stream, dev, K=10, horizon=8):
     return grad, comp
 
 
-def large_species_case(args, dev, stream, flush):
-    """The large single-GPU case measured beside the headline: 3D Euler + species transport (5 NASA-7
-    species), 256^3 periodic-x shear layer, AusmpUp, least squares + minmod. FP64 RHS, the mixed request,
-    JVP and VJP with the headline's protocol (L2 flushed between steps, CUDA events), and the FP64
-    residual against the oracle's on the same state."""
+def species_workload_case(args, dev, stream, flush, name, n):
+    """A species configuration measured beside the headline, with the headline's protocol (L2 flushed
+    between steps, CUDA events): the FP64 RHS, the mixed request, the JVP and the VJP, and the FP64
+    residual against the oracle's on the same state. `shear3d` at 256: 3D Euler + 5 NASA-7 species,
+    256^3 shear layer, AusmpUp, least squares + minmod (the large single-GPU case). `channel_tets` at
+    2,000,000: Navier-Stokes + 9 NASA-7 species with constant-Lewis transport on Delaunay tetrahedra
+    in a 1 x 0.2 x 0.2 channel."""
     import torch
     from ablate_b200 import _lib as L
     from ablate_b200.workloads import initial_aux
     from oracle import oracle as orc
 
     t_setup = time.perf_counter()
-    w = make_workload("shear3d", 256)
+    w = make_workload(name, n)
     solver = w.solver(device=dev.index)
     aux0 = initial_aux(w)
     solver.SetAux(aux0)
@@ -705,13 +707,15 @@ def main():
         line["parity"] = parity
     solver.close()
     if world == 1 and w.name == "tgv3d" and not args.no_species_case:
-        # the large single-GPU species case (its own line key; the headline above stays the 128^3 case)
+        # the species configurations, each under its own line key (the headline above stays the 128^3 case)
         del U, F
         torch.cuda.empty_cache()
-        try:
-            line["species_case"] = large_species_case(args, dev, stream, flush)
-        except Exception as e:  # reported, the headline line stands
-            line["species_case"] = {"error": f"{type(e).__name__}: {e}"}
+        for key, name, n in (("species_case", "shear3d", 256), ("tets_case", "channel_tets", 2_000_000)):
+            try:
+                line[key] = species_workload_case(args, dev, stream, flush, name, n)
+            except Exception as e:  # reported, the headline line stands
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
