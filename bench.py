@@ -14,6 +14,9 @@ Device times come from CUDA events around each step on the launching stream, L2 
 steps, max over ranks.
 ``--impl reference`` times the CPU restatement of the reference algorithm (the oracle; the reference
 itself needs PETSc/MPI/TChem, absent here) on all host cores, rank 0 only.
+At N = 1 the default run also measures two species configurations under their own keys
+(``species_case``: 256^3, five NASA-7 species; ``tets_case``: 2M tetrahedra, nine species): RHS, JVP,
+VJP and the FP64 error against the oracle at full size. ``--no-species-case`` skips them.
 """
 from __future__ import annotations
 
