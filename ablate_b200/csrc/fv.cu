@@ -41,6 +41,13 @@ bool fused_enabled() {
     return v && v[0] == '1';
 }
 
+// the mixed path with species (the exact instances up to 9 species) when ABL_FV_MIXED_SPECIES=1 at
+// create; by default a mixed request with species runs the FP64 kernels
+bool mixed_species_enabled() {
+    const char* v = std::getenv("ABL_FV_MIXED_SPECIES");
+    return v && v[0] == '1';
+}
+
 int fail(const AblError& e) {
     g_last_error = e.what();
     return e.code;
@@ -508,6 +515,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         fv->naux = 1 + h.dim + fv->ns;
         fv->ns_user = ns_user;
         fv->pad = pad;
+        fv->mixed_species = mixed_species_enabled() && fv->ns > 0 && fv->ns <= 9;
         fv->nc_user = fv->nc - pad;
         fv->naux_user = fv->naux - pad;
         fv->n_cells = h.n_cells;
@@ -584,7 +592,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
                 fv->n_geo_classes = (int)ntf;
             }
             fv->tf_geo.upload(geo.data(), geo.size());
-            if (fv->ns == 0) {
+            if (fv->ns == 0 || fv->mixed_species) {
                 std::vector<double> g32(6 * ntf, 0.0);
                 for (size_t i = 0; i < ntf; i++) {
                     for (int d = 0; d < 3; d++) g32[6 * i + d] = geo[10 * i + d];
@@ -645,7 +653,7 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
             fv->cwa.upload(cwa.data(), cwa.size());
             fv->cv.upload(cv.data(), cv.size());
             fv->cwar.upload(cwar.data(), cwar.size());
-            if (fv->ns == 0) {  // the mixed path's copies (with species it runs the FP64 kernels)
+            if (fv->ns == 0 || fv->mixed_species) {  // the mixed path's copies (with species by default it runs the FP64 kernels)
                 const size_t nw = cwa.size() / 6;
                 std::vector<float> f32(8 * nw, 0.0f);
                 for (size_t i = 0; i < nw; i++)
@@ -716,11 +724,11 @@ int abl_fv_create(const abl_mesh_desc* mesh, const abl_physics_desc* physics, in
         }
         if (lsq) {
             fv->grad64.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 2));
-            if (fv->ns == 0) fv->grad32.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 4));
+            if (fv->ns == 0 || fv->mixed_species) fv->grad32.alloc((size_t)fv->n_cells * round_up(fv->nc * fv->dim, 4));
         }
         if (dif) {
             fv->agrad64.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 2));
-            if (fv->ns == 0) fv->agrad32.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 4));
+            if (fv->ns == 0 || fv->mixed_species) fv->agrad32.alloc((size_t)fv->n_cells * round_up(fv->naux * fv->dim, 4));
         }
         fv->status.alloc(1);
         fv->status.zero();

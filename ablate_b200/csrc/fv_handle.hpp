@@ -102,6 +102,8 @@ struct abl_fv {
     abl::DevBuf<int> fz_ext_ptr, fz_ext, fz_tile_cls, fz_cls_off, fz_pool;
     int fz_max_ext = 0, fz_max_grad = 0, fz_max_faces = 0, fz_classes = 0;
     bool fused_ok[2] = {false, false};
+    // a mixed request with species runs the FP32-gradient kernels (ABL_FV_MIXED_SPECIES=1 at create)
+    bool mixed_species = false;
     size_t fused_smem[2] = {0, 0};
     int n_sm = 1;
     // optional per-kernel timing of the last evaluation

@@ -166,12 +166,12 @@ void run_rhs(abl_fv* fv, const double* U, double* F, int precision, int overwrit
         mark(fv, "k_aux", s);
         launch_aux<DIM, NS>(fv, U, s);
     }
-    // With species the mixed request runs the FP64 kernels: the NASA-7 decode (FP64 by design) dominates
-    // their cost, and FP32 gradients of steep temperature / composition layers exceed the 1e-6 error
-    // budget (1.2e-6 on the 2M-tetrahedron channel).
+    // With species a mixed request runs the FP64 kernels unless the handle was created with
+    // ABL_FV_MIXED_SPECIES=1: the NASA-7 decode (FP64 by design) dominates their cost (the FP32-gradient
+    // kernels gain 2-6 %), and on the 2M-tetrahedron channel their error reaches 1.2e-6 against FP64.
     bool done = false;
-    if constexpr (NS == 0) {
-        if (precision == ABL_PRECISION_MIXED) {
+    if constexpr (kSpecialized<NS>) {
+        if (precision == ABL_PRECISION_MIXED && (NS == 0 || fv->mixed_species)) {
             rhs_with<DIM, NS, float>(fv, U, fv->grad32.p, fv->agrad32.p, F, overwrite, s);
             done = true;
         }

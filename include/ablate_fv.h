@@ -102,7 +102,9 @@ extern "C" {
 
 /* precision of abl_fv_rhs */
 #define ABL_PRECISION_FP64 0
-#define ABL_PRECISION_MIXED 1 /* FP32 reconstruction/flux arithmetic, FP64 e=E/rho-|u|^2/2, T solve and accumulation */
+#define ABL_PRECISION_MIXED 1 /* FP32 reconstruction/flux arithmetic, FP64 e=E/rho-|u|^2/2, T solve and accumulation.
+                                With species a mixed request runs the FP64 kernels, unless ABL_FV_MIXED_SPECIES=1
+                                is set at abl_fv_create (instances up to 9 species) */
 /* or'ed into the precision argument of abl_fv_rhs: F = RHS(U) instead of F += RHS(U) (for a caller
  * whose residual vector holds nothing else; saves reading F) */
 #define ABL_RHS_OVERWRITE 0x100

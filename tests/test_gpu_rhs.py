@@ -126,3 +126,27 @@ def test_tiny_and_ragged_meshes_match_the_oracle(shape, periodic):
     scale = np.linalg.norm(F_ref[owned])
     assert np.linalg.norm(F[owned] - F_ref[owned]) <= FP64_TOL * max(scale, 1e-300)
     assert np.all(F[~owned] == 0.0)
+
+
+@pytest.mark.parametrize("name", ["species3d_ns5", "species3d_ns9", "tets3d_ns9", "shear3d_ns5", "pgspecies3d_ns2"])
+def test_rhs_mixed_with_species_opt_in(name):
+    # ABL_FV_MIXED_SPECIES=1 at create runs the FP32-gradient kernels for a mixed request with species
+    # (by default such a request runs the FP64 kernels); on these cases they stay within the mixed bar
+    import os
+    w = R.case(name)
+    F64, _ = _run(w, L.PRECISION_FP64)
+    old = os.environ.get("ABL_FV_MIXED_SPECIES")
+    os.environ["ABL_FV_MIXED_SPECIES"] = "1"
+    try:
+        F32, _ = _run(w, L.PRECISION_MIXED)
+    finally:
+        if old is None:
+            del os.environ["ABL_FV_MIXED_SPECIES"]
+        else:
+            os.environ["ABL_FV_MIXED_SPECIES"] = old
+    Fdef, _ = _run(w, L.PRECISION_MIXED)
+    owned = w.mesh.cell_kind == L.CELL_OWNED
+    assert np.array_equal(Fdef, F64), "without the switch a mixed request with species runs the FP64 kernels"
+    assert not np.array_equal(F32, F64), "with the switch the FP32-gradient kernels run"
+    for block, e in R.block_errors(F32, F64, owned, 2 + w.mesh.dim).items():
+        assert e <= MIXED_TOL, f"{name} {block}: {e:.3e}"
