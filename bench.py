@@ -353,7 +353,7 @@ def species_workload_case(args, dev, stream, flush, name, n):
     n = out["n_cells"]
     out["fp64"] = {"ms_per_step": ms["fp64"], "mcell_per_s": n / (ms["fp64"] * 1e-3) / 1e6, "hbm_gbs": B / (ms["fp64"] * 1e-3) / 1e9}
     out["mixed"] = {"ms_per_step": ms["mixed"], "mcell_per_s": n / (ms["mixed"] * 1e-3) / 1e6,
-                    "note": "with species the mixed request runs the FP64 kernels (FP32 species gradients measured above 1e-6 relative)"}
+                    "note": "with species a mixed request runs the FP64 kernels unless ABL_FV_MIXED_SPECIES=1 is set at create (the FP32-gradient kernels measured 1.18e-6 against FP64 on the 2M tetrahedra and 1.02-1.06x faster)"}
     out["jvp"] = {"ms_per_step": ms["jvp"], "over_rhs_fp64": ms["jvp"] / ms["fp64"]}
     out["vjp"] = {"ms_per_step": ms["vjp"], "over_rhs_fp64": ms["vjp"] / ms["fp64"],
                   "note": "limiter and EOS recomputed inside the VJP (no intermediates kept from a forward pass)"}
