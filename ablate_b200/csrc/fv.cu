@@ -148,9 +148,10 @@ void upload_species(const abl_physics_desc* p, Phys& P, DevBuf<double>& nasa7, D
 
 // ---- dispatch over the compiled (DIM, NS) instances ------------------------------------------------
 // Exact species counts (fv_inst_a..d.cu, fv_adj_*.cu), the 16-species instances (fv_inst_e.cu,
-// fv_inst_f.cu: RHS, aux update, tangent) and the kMaxSpecies capacity instances (fv_inst_cap.cu: RHS
+// fv_inst_f.cu: RHS, aux update, tangent), the 3D 64-species instance (fv_inst_g.cu: RHS and aux update,
+// fv_inst_h.cu: tangent; run-time loops) and the kMaxSpecies capacity instances (fv_inst_cap.cu: RHS
 // and aux update, run-time loops), per dimension, ascending.
-constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSpecies, -1}, {0, 2, 3, 5, 9, 16, kMaxSpecies, -1}};
+constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSpecies, -1}, {0, 2, 3, 5, 9, 16, 64, kMaxSpecies}};
 
 #define ABL_CASES_EXACT(FN, ...)                              \
     case 1000: FN<1, 0>(fv, __VA_ARGS__); break;              \
@@ -165,6 +166,8 @@ constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSp
     case 1016: FN<1, 16>(fv, __VA_ARGS__); break;             \
     case 2016: FN<2, 16>(fv, __VA_ARGS__); break;             \
     case 3016: FN<3, 16>(fv, __VA_ARGS__); break;
+#define ABL_CASES_64(FN, ...) \
+    case 3064: FN<3, 64>(fv, __VA_ARGS__); break;
 #define ABL_CASES_CAP(FN, ...)                                \
     case 1000 + kMaxSpecies: FN<1, kMaxSpecies>(fv, __VA_ARGS__); break; \
     case 2000 + kMaxSpecies: FN<2, kMaxSpecies>(fv, __VA_ARGS__); break; \
@@ -176,6 +179,7 @@ constexpr int kInstances[3][8] = {{0, 16, kMaxSpecies, -1}, {0, 2, 3, 16, kMaxSp
         switch ((fv)->dim * 1000 + (fv)->ns) {                                                                            \
             ABL_CASES_EXACT(FN, __VA_ARGS__)                                                                              \
             ABL_CASES_16(FN, __VA_ARGS__)                                                                                 \
+            ABL_CASES_64(FN, __VA_ARGS__)                                                                                 \
             ABL_CASES_CAP(FN, __VA_ARGS__)                                                                                \
             default: throw AblError(ABL_ERR_UNSUPPORTED, "no compiled RHS instance for this dimension/species count"); \
         }                                                                                                                 \
@@ -200,9 +204,10 @@ void dispatch_jvp(abl_fv* fv, const double* U, const double* dU, double* F, doub
     switch (fv->dim * 1000 + fv->ns) {
         ABL_CASES_EXACT(run_jvp, U, dU, F, dF, s)
         ABL_CASES_16(run_jvp, U, dU, F, dF, s)
+        ABL_CASES_64(run_jvp, U, dU, F, dF, s)
         default:
-            throw AblError(ABL_ERR_UNSUPPORTED, "the JVP is compiled for up to 16 species; " + std::to_string(fv->ns_user) + " species run in the " +
-                                                    std::to_string(fv->ns) + "-species instance, which has the RHS only");
+            throw AblError(ABL_ERR_UNSUPPORTED, "the JVP is compiled for up to 16 species (64 in 3D); " + std::to_string(fv->ns_user) +
+                                                    " species run in the " + std::to_string(fv->ns) + "-species instance, which has the RHS only");
     }
 }
 

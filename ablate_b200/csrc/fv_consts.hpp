@@ -11,6 +11,16 @@
 #define ABL_UNROLL_SPECIES _Pragma("unroll")
 #endif
 
+// The loops of the NASA-7 mixture functions (the mass fractions, e_s, cp, the molar mass) follow the
+// species loops, except in the unit of the 64-species tangent (ABL_CAPACITY_UNROLL_MIXTURE), which
+// keeps them unrolled: built with those loops at run time, the capacity instances' tangent kernels
+// returned NaN where their RHS was exact, and unrolled at 64 species they compile in minutes.
+#if defined(ABL_CAPACITY_TU) && !defined(ABL_CAPACITY_UNROLL_MIXTURE)
+#define ABL_UNROLL_MIXTURE _Pragma("unroll 1")
+#else
+#define ABL_UNROLL_MIXTURE _Pragma("unroll")
+#endif
+
 namespace abl {
 
 // Faces per colour in a tile (the adjoint kernel runs one colour per pass, two lanes per face, on

@@ -477,7 +477,7 @@ template <class S>
 ABL_HD void fill_y(int ns, S rho, const S* rhoY, S* ys) {
     S sum = 0.0;
     const S irho = rcp64(rho);
-ABL_UNROLL_SPECIES
+ABL_UNROLL_MIXTURE
     for (int s = 0; s < ns - 1; s++) {
         S y = pmax(S(0.0), rhoY[s] * irho);
         y = pmin(S(1.0), y);
@@ -485,7 +485,7 @@ ABL_UNROLL_SPECIES
         sum += y;
     }
     if (sum > 1.0) {
-ABL_UNROLL_SPECIES
+ABL_UNROLL_MIXTURE
         for (int s = 0; s < ns - 1; s++) ys[s] /= sum;
         ys[ns - 1] = 0.0;
     } else {
@@ -498,7 +498,7 @@ ABL_UNROLL_SPECIES
 template <class S, class ST>
 ABL_HD S e_sens(const Phys& P, int ns, const S* ys, ST T) {
     S e = 0;
-ABL_UNROLL_SPECIES
+ABL_UNROLL_MIXTURE
     for (int k = 0; k < ns; k++) e += (nasa_h_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k] - P.href[k] - kRuniv * T * P.inv_mw[k]) * ys[k];
     return e;
 }
@@ -543,14 +543,14 @@ ABL_HD double nasa_temperature(const Phys& P, int ns, const double* ys, double e
 template <class S>
 ABL_HD S mixture_cp(const Phys& P, int ns, const S* ys, S T) {
     S cp = 0;
-ABL_UNROLL_SPECIES
+ABL_UNROLL_MIXTURE
     for (int k = 0; k < ns; k++) cp += ys[k] * nasa_cp_molar(P.nasa7 + 15 * k, T) * P.inv_mw[k];
     return cp;
 }
 template <class S>
 ABL_HD S mixture_mw(const Phys& P, int ns, const S* ys) {
     S iw = 0;
-ABL_UNROLL_SPECIES
+ABL_UNROLL_MIXTURE
     for (int k = 0; k < ns; k++) iw += ys[k] * P.inv_mw[k];
     return rcp64(iw);
 }

@@ -138,12 +138,13 @@ typedef struct abl_physics_desc {
     int32_t n_species;       /* densityYi components, 0..128; 0 = no species field. Instances with their
                                 loops unrolled: (1, 0), (2, 0), (2, 2), (2, 3), (3, 0), (3, 2), (3, 5),
                                 (3, 9) (every entry point); 16 species in 1D, 2D and 3D (RHS, JVP, aux);
-                                with run-time loops, 128 species in 1D, 2D and 3D (RHS, aux). Any other
+                                with run-time loops, 64 species in 3D (RHS, JVP, aux) and 128 species in
+                                1D, 2D and 3D (RHS, aux). Any other
                                 count runs in the smallest instance that holds it, its species after zero-state
                                 padding species (results unchanged; the RHS, JVP, VJP and aux entry points
                                 translate the rows). An entry point the instance does not compile returns
                                 ABL_ERR_UNSUPPORTED: the VJP above 9 species (3 in 2D, none with species in
-                                1D), the JVP above 16, the ghost, step, CFL, normalisation and functional
+                                1D), the JVP above 16 (64 in 3D), the ghost, step, CFL, normalisation and functional
                                 entry points for counts other than the exact ones */
     const double* nasa7;     /* [n_species][15]: T_mid, low a1..a7, high a1..a7 (cp/R = a1 + a2 T + ... ) */
     const double* mw;        /* [n_species] molar mass kg/kmol */

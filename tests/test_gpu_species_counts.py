@@ -1,6 +1,7 @@
 """Any species count. The kernels are compiled for a few exact counts (0, 2, 3 in 2D; 0, 2, 5 and 9 in
-3D), for 16 species (RHS, aux update and tangent, unrolled) and for a capacity of 128 species (RHS and aux
-update, loops over the state components at run time); a count without an instance of its own runs in
+3D), for 16 species (RHS, aux update and tangent, unrolled), for 64 species in 3D (RHS, aux update and
+tangent, loops over the state components at run time) and for a capacity of 128 species (RHS and aux
+update, run-time loops); a count without an instance of its own runs in
 the smallest instance that holds it, its species after zero-state padding species, and every entry point
 of the RHS and its derivatives translates the rows (the species padding in ablate_b200/csrc/fv.cu).
 ABL_FV_SPECIES_INSTANCE at create asks for a larger instance than needed, so that an exact count can be
@@ -8,10 +9,11 @@ run padded and compared with itself.
 
 Checked: the RHS at 1, 4, 7 and 12 synthetic NASA-7 species and at the 53 species of the reference's
 gri30 mechanism against the oracle (1e-12); the RHS, JVP and VJP of 5 species padded into the 9-species
-instance, its RHS and JVP padded into the 16-species instance and its RHS padded into the 128-species one,
-against the exact 5-species instance; the refusals of the derivatives an instance does not compile; the
-VJP as the transpose of the JVP on padded counts; the reference's 1D three-species diffusion convergence
-test on the device.
+instance, its RHS and JVP padded into the 16- and 64-species instances and its RHS padded into the
+128-species one, against the exact 5-species instance; the refusals of the derivatives an instance does
+not compile; the VJP as the transpose of the JVP on padded counts; the JVP of 12 species and of gri30's
+53 against central differences; the reference's 1D three-species diffusion convergence test on the
+device.
 """
 import os
 
@@ -85,7 +87,7 @@ def _derivatives(s, w, seed, jvp=True, vjp=True):
     return [F] + ([dF] if jvp else []) + ([Ub] if vjp else [])
 
 
-@pytest.mark.parametrize("instance,jvp,vjp", [(9, True, True), (16, True, False), (128, False, False)])
+@pytest.mark.parametrize("instance,jvp,vjp", [(9, True, True), (16, True, False), (64, True, False), (128, False, False)])
 def test_padded_instance_equals_the_exact_instance(instance, jvp, vjp):
     # five species have an instance of their own; run padded they must give the same RHS and the same
     # derivatives where the instance compiles them (the others are refused with ERR_UNSUPPORTED)
@@ -145,6 +147,26 @@ def test_jvp_of_a_count_in_the_16_species_instance_matches_finite_differences():
     s.close()
     fd = (Fp - Fm) / (2 * eps)
     assert np.linalg.norm(Jv[owned] - fd[owned]) <= 1e-5 * np.linalg.norm(fd[owned])
+
+
+def test_jvp_of_gri30_in_the_64_species_instance_matches_finite_differences():
+    # the 53 species of gri30 run in the 64-species instance: the tangent against a central difference
+    w = R.case("gri30_box3d")
+    s = _solver(w)
+    owned = w.mesh.cell_kind == L.CELL_OWNED
+    rng = np.random.default_rng(5)
+    v = rng.standard_normal(w.U.shape) * np.abs(w.U).mean(0)
+    v[~owned] = 0.0
+    Jv = s.ComputeJVP(0.0, w.U, v, np.zeros_like(w.U))
+    eps = 1e-6
+    Fp, Fm = np.zeros_like(w.U), np.zeros_like(w.U)
+    s.ComputeRHSFunction(0.0, w.U + eps * v, Fp, L.PRECISION_FP64)
+    s.ComputeRHSFunction(0.0, w.U - eps * v, Fm, L.PRECISION_FP64)
+    assert s.Status() == L.OK
+    s.close()
+    fd = (Fp - Fm) / (2 * eps)
+    assert np.all(np.isfinite(Jv))
+    assert np.linalg.norm(Jv[owned] - fd[owned]) <= 1e-6 * np.linalg.norm(fd[owned])
 
 
 def test_stepping_entry_points_need_a_count_with_its_own_instance():
